@@ -1,0 +1,320 @@
+#!/usr/bin/env python3
+"""Benchmark: Kerr rays/s of the 1024x1024, 4-spp thin-disk render.
+
+Workload (one step = one full frame): Kerr a=0.998, M=1, observer r=50,
+theta=80 deg, phi=0, horizontal FOV 90 deg; thin disk ISCO..20 M,
+T_peak 1e7 K, blackbody chromaticity with redshift and g^4 beaming; star
+background (5000 stars, seed 42); adaptive Dormand-Prince 5(4) at tolerance
+1e-8, at most 10000 steps; 2x2 stratified jitter from the reference's hash.
+1024*1024*4 = 4,194,304 rays per step. Inputs are synthetic (the scene is
+generated from its parameters; no dataset).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|mixed]
+  python bench.py --impl reference   # the reference's own CPU code, same workload
+
+`value` is rays/s with the scene and the output resident on the device (CUDA
+events around each render launch on its stream; a 256 MiB buffer is written
+between steps to flush the 126 MB L2). `e2e` is the same metric through the
+reference C entry point grrt_render with a host framebuffer (launch
+parameters in, the float RGBA frame out, every step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Kerr rays/s at 1024^2: plain FP64 vs mixed vs surrogate at <=1e-4 rel intensity"
+WORKLOAD = "kerr_a0.998_1024x1024_4spp_thin_disk_isco_20M_stars_seed42_tol1e-8"
+W = H = 1024
+SPP = 4
+RAYS = W * H * SPP
+
+# Algorithmic FLOPs of the reference method (binary + - * / and sqrt, counted
+# in the reference source; transcendental calls counted apart):
+#   one Kerr right-hand side (include/grrt/spacetime/kerr.h:31-109): 133
+#   fast_sincos (include/grrt/math/fast_trig.h:21-82): 37
+#   one DP45 attempt (include/grrt/geodesic/rk4.h:73-177): 7 right-hand sides
+#   + 480 for the stage sums, the 5th-order solution and the error norm over
+#   the reference's 8-component state
+F_EVAL = 133 + 37
+F_ATTEMPT = 7 * F_EVAL + 480
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# peaks
+# ---------------------------------------------------------------------------
+def measured_peaks(torch) -> dict:
+    peaks = {}
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        peaks.update(json.load(open(path)))
+    # FP64 roofline denominator: cuBLAS DGEMM measured here (the same method
+    # the driver uses for its bf16 figure), best of 5.
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    peaks["fp64_tflops_dgemm"] = best
+    return peaks
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU implementation (oracle/_ref, built from its own sources)
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(row_offset: int = 0, stride: int = 16):
+    """Render rows row_offset, row_offset+stride, ... of the benchmark frame with
+    the reference's own code (as-shipped optimisation flags) on all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import grrt_b200 as G
+    import oracle_bind
+    kind = "fast" if oracle_bind.ref_available("fast") else "strict"
+    ref = oracle_bind.RefScene(G.config_params(2), kind=kind)
+    _, secs, threads = ref.render_rows(row_offset, stride)
+    rows = len(range(row_offset, H, stride))
+    rays = rows * W * SPP
+    return rays, secs, threads, kind, rows
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    stride = 16
+    for w in range(args.warmup):
+        cpu_reference_sample(w % stride, stride * 4)
+    total_rays, total_secs, threads, kind, rows = 0, 0.0, 1, "fast", 0
+    for k in range(args.steps):
+        rays, secs, threads, kind, rows = cpu_reference_sample(k % stride, stride)
+        total_rays += rays
+        total_secs += secs
+    value = total_rays / total_secs
+    sample = (f"every {stride}th row of the 1024x1024 4-spp frame ({rows} rows, {rows * W * SPP} rays) per step, "
+              f"row offset = step mod {stride}; reference src/*.cpp built with its shipped flags "
+              f"(minus -march=native and LTO), OpenMP over all host threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP},
+            "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads,
+                             "kind": "reference" if kind else "port", "sample": sample},
+            "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import grrt_b200 as G
+
+    form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
+    R = G.Renderer(G.config_params(2))
+    R.set_precision(form)
+    stream = torch.cuda.Stream()
+    rgba = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step(timed_events=None):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # evict L2 between frames
+            if timed_events is not None:
+                timed_events[0].record(stream)
+            R.render_device(rgba, None, None, stream)
+            if timed_events is not None:
+                timed_events[1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    st = R.stats()
+    attempts_per_frame = st["attempts"]
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(evs[k])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    kernel_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = float(np.mean(kernel_ms))
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * RAYS / (ms * 1e-3)
+
+    # end to end through the reference C entry point (host framebuffer)
+    host_fb = np.empty((H, W, 4), dtype=np.float32)
+    import ctypes as C
+    L = G.lib()
+    fbp = host_fb.ctypes.data_as(C.POINTER(C.c_float))
+    for _ in range(2):
+        L.grrt_render(R.ctx, fbp)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        rc = L.grrt_render(R.ctx, fbp)
+        assert rc == 0, L.grrt_error(R.ctx)
+    e2e_s = (time.perf_counter() - e0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * RAYS / e2e_s, "unit": "rays/s",
+           "h2d_bytes_per_step": 1536,  # launch parameters (scene description) per frame
+           "d2h_bytes_per_step": W * H * 16,  # float RGBA frame
+           "api": "grrt_render(ctx, float* host_framebuffer)", "ms_per_step": 1e3 * e2e_s}
+
+    line = None
+    if rank == 0:
+        peaks = measured_peaks(torch)
+        peak = peaks["fp64_tflops_dgemm"]
+        flops = attempts_per_frame * F_ATTEMPT
+        achieved = flops / (ms * 1e-3) / 1e12
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (best of 5); MEASURED_PEAKS.json "
+                               "has no FP64 figure",
+                "flops_per_launch": flops, "flop_count": f"{F_ATTEMPT} per DP45 attempt x {attempts_per_frame} "
+                                                        f"attempts (device counter)",
+                "traffic": None, "kernel": "thin_render_kernel<0>"}
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                rays, secs, threads, kind, rows = cpu_reference_sample(0, 16)
+                cpu = {"value": rays / secs, "unit": "rays/s", "cores": threads, "kind": "reference",
+                       "sample": f"rows 0,16,...,1008 of the same frame ({rows * W * SPP} rays), reference "
+                                 f"src/*.cpp ({kind} build) via oracle/_ref, OpenMP, {secs:.2f} s"}
+            except Exception as ex:  # the baseline is reported, not required
+                cpu = {"value": None, "unit": "rays/s", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {ex}"}
+        line = {"metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if form == G.FORM_FP64 else "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "rays_per_step": RAYS,
+                           "form": args.form, "l2": "flushed between steps (256 MiB write)",
+                           "parallelism": f"one frame per GPU per step ({world} GPU)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": args.steps,
+                "work": {"attempts_per_ray": attempts_per_frame / RAYS, "accepted_per_ray": st["accepted"] / RAYS,
+                         "crossings": st["crossings"], "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])},
+                "kernel_ms_per_step": kernel_ms, "wall_s_timed_region": wall}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,309 @@
+"""grrt_b200 — Python binding of libgrrt.so, the B200-native GRRT renderer.
+
+The library exports the reference's pure C API unchanged (include/grrt_api.h:
+grrt_create / grrt_render* / grrt_destroy, GRRTParams) plus additive entry
+points (include/grrt_b200.h). This module binds both with ctypes so Python
+callers (tests, bench.py) use exactly the C ABI a C/C++ host would.
+
+Every render runs on the GPU through the sm_100a kernels in
+grrt_b200/csrc/device; there is no CPU fallback. Importing this module fails
+loudly if the shared library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "GRRTParams", "GRRTStats", "Renderer", "lib", "load_library", "build",
+    "FORM_FP64", "FORM_MIXED", "config_params", "LIB_PATH",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgrrt.so")
+
+FORM_FP64 = 0
+FORM_MIXED = 1
+
+METRIC_SCHWARZSCHILD = 0
+METRIC_KERR = 1
+BG_BLACK = 0
+BG_STARS = 1
+BG_TEXTURE = 2
+
+
+class GRRTParams(C.Structure):
+    """Mirror of GRRTParams (include/grrt/types.h:20-64, include/grrt_api.h)."""
+
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int),
+        ("metric_type", C.c_int), ("mass", C.c_double), ("spin", C.c_double),
+        ("observer_r", C.c_double), ("observer_theta", C.c_double), ("observer_phi", C.c_double),
+        ("fov", C.c_double),
+        ("cam_yaw", C.c_double), ("cam_pitch", C.c_double), ("cam_roll", C.c_double),
+        ("disk_enabled", C.c_int), ("disk_inner", C.c_double), ("disk_outer", C.c_double),
+        ("disk_temperature", C.c_double),
+        ("disk_volumetric", C.c_int), ("disk_alpha", C.c_double), ("disk_turbulence", C.c_double),
+        ("disk_seed", C.c_int), ("disk_noise_scale", C.c_double), ("disk_noise_octaves", C.c_int),
+        ("mass_solar", C.c_double), ("eddington_fraction", C.c_double),
+        ("background_type", C.c_int), ("background_texture_path", C.c_char_p),
+        ("integrator_tolerance", C.c_double), ("integrator_max_steps", C.c_int),
+        ("samples_per_pixel", C.c_int), ("thread_count", C.c_int), ("backend", C.c_int),
+        ("num_frequency_bins", C.c_int), ("frequency_bins_hz", C.POINTER(C.c_double)),
+    ]
+
+
+class GRRTStats(C.Structure):
+    """Mirror of GRRTStats (include/grrt_b200.h)."""
+
+    _fields_ = [
+        ("attempts", C.c_ulonglong), ("accepted", C.c_ulonglong), ("crossings", C.c_ulonglong),
+        ("rays", C.c_ulonglong), ("horizon", C.c_ulonglong), ("escaped", C.c_ulonglong),
+        ("max_steps", C.c_ulonglong), ("clamp_evals", C.c_ulonglong), ("march_steps", C.c_ulonglong),
+        ("physics_steps", C.c_ulonglong), ("bin_updates", C.c_ulonglong),
+        ("fp64_attempts", C.c_ulonglong), ("kernel_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_float, C.c_void_p)
+
+_lib: Optional[C.CDLL] = None
+
+
+def build(jobs: int = 8) -> None:
+    """Compile libgrrt.so in-tree (host C++ and sm_100a CUDA)."""
+    import subprocess
+    subprocess.run(["make", "-j", str(jobs)], cwd=os.path.join(_HERE, "csrc"), check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libgrrt.so and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libgrrt.so not built ({path}); run grrt_b200.build() or make -C grrt_b200/csrc")
+    L = C.CDLL(path)
+    P = C.POINTER
+    vp = C.c_void_p
+    sig = {
+        "grrt_create": (vp, [P(GRRTParams)]),
+        "grrt_destroy": (None, [vp]),
+        "grrt_update_params": (None, [vp, P(GRRTParams)]),
+        "grrt_render": (C.c_int, [vp, P(C.c_float)]),
+        "grrt_render_cb": (C.c_int, [vp, P(C.c_float), PROGRESS_FN, vp]),
+        "grrt_render_tile": (C.c_int, [vp, P(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int]),
+        "grrt_cancel": (None, [vp]),
+        "grrt_progress": (C.c_float, [vp]),
+        "grrt_error": (C.c_char_p, [vp]),
+        "grrt_cuda_available": (C.c_int, []),
+        "grrt_last_error": (C.c_char_p, []),
+        "grrt_tonemap": (None, [P(C.c_float), C.c_int, C.c_int]),
+        "grrt_debug_pixel": (None, [vp, C.c_int, C.c_int]),
+        "grrt_set_frequency_bins": (None, [vp, P(C.c_double), C.c_int]),
+        "grrt_render_spectral": (C.c_int, [vp, P(C.c_double), C.c_int, C.c_int]),
+        "grrt_render_spectral_cb": (C.c_int, [vp, P(C.c_double), C.c_int, C.c_int, PROGRESS_FN, vp]),
+        "grrt_render_spectral_to_fits_cb": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_int, PROGRESS_FN, vp]),
+        "grrt_set_precision": (C.c_int, [vp, C.c_int]),
+        "grrt_get_precision": (C.c_int, [vp]),
+        "grrt_set_mixed_params": (C.c_int, [vp, C.c_double, C.c_double]),
+        "grrt_render_device": (C.c_int, [vp, vp, vp, vp, vp]),
+        "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
+        "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
+        "grrt_scene_table": (C.c_longlong, [vp, C.c_char_p, P(C.c_double), C.c_longlong]),
+        "grrt_camera_ray": (C.c_int, [vp, C.c_double, C.c_double, P(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def lib() -> C.CDLL:
+    return load_library()
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def config_params(config: int = 1, *, width: Optional[int] = None, height: Optional[int] = None,
+                  spp: Optional[int] = None, **overrides) -> dict:
+    """GRRTParams field values of the benchmark scenes.
+
+    1: Schwarzschild (M=1) 256x256, 1 spp, thin disk ISCO..20, black background.
+    2: Kerr a=0.998 1024x1024, 4 spp, thin disk ISCO..20, stars (seed 42).
+    3: volumetric Kerr a=0.9 512x512, 1 spp, alpha 0.1, turbulence 0.4, 2 octaves,
+       seed 42, outer 20, M=10 M_sun at 0.1 Eddington; 32 log-spaced bins 1e14..1e18 Hz.
+    Observer r=50, theta=80 deg, phi=0, FOV 90 deg, tolerance 1e-8, 10000 steps.
+    """
+    p = dict(width=256, height=256, metric_type=METRIC_KERR, mass=1.0, spin=0.998, observer_r=50.0,
+             observer_theta=math.radians(80.0), observer_phi=0.0, fov=math.radians(90.0),
+             disk_enabled=1, disk_inner=0.0, disk_outer=20.0, disk_temperature=0.0, disk_volumetric=0,
+             disk_alpha=0.1, disk_turbulence=0.4, disk_seed=42, disk_noise_scale=0.0,
+             disk_noise_octaves=2, mass_solar=0.0, eddington_fraction=0.0, background_type=BG_STARS,
+             integrator_tolerance=1e-8, integrator_max_steps=10000, samples_per_pixel=1)
+    if config == 1:
+        p.update(metric_type=METRIC_SCHWARZSCHILD, spin=0.0, background_type=BG_BLACK)
+    elif config == 2:
+        p.update(width=1024, height=1024, samples_per_pixel=4)
+    elif config == 3:
+        p.update(width=512, height=512, spin=0.9, disk_volumetric=1, mass_solar=10.0,
+                 eddington_fraction=0.1, background_type=BG_BLACK)
+    else:
+        raise ValueError(f"unknown config {config}")
+    if width is not None:
+        p["width"] = width
+    if height is not None:
+        p["height"] = height
+    if spp is not None:
+        p["samples_per_pixel"] = spp
+    p.update(overrides)
+    return p
+
+
+def log_bins(lo: float = 1e14, hi: float = 1e18, n: int = 32) -> np.ndarray:
+    """n log-spaced frequencies in [lo, hi] (the CLI's --freq-range)."""
+    if n == 1:
+        return np.array([lo], dtype=np.float64)
+    llo, lhi = math.log10(lo), math.log10(hi)
+    return np.array([10.0 ** (llo + (lhi - llo) * i / (n - 1)) for i in range(n)], dtype=np.float64)
+
+
+def make_params(values: dict, freqs: Optional[np.ndarray] = None) -> GRRTParams:
+    p = GRRTParams()
+    for k, v in values.items():
+        if k in ("frequency_bins_hz", "num_frequency_bins"):
+            continue
+        setattr(p, k, v)
+    if freqs is not None:
+        p.num_frequency_bins = len(freqs)
+        p.frequency_bins_hz = _dptr(freqs)
+    return p
+
+
+class Renderer:
+    """One GRRT context (grrt_create ... grrt_destroy)."""
+
+    def __init__(self, values: Optional[dict] = None, freqs: Optional[Sequence[float]] = None, **kw):
+        self._L = lib()
+        vals = dict(values or {})
+        vals.update(kw)
+        self.values = vals
+        self.freqs = None if freqs is None else np.ascontiguousarray(freqs, dtype=np.float64)
+        params = make_params(vals, self.freqs)
+        self.ctx = self._L.grrt_create(C.byref(params))
+        if not self.ctx:
+            err = self._L.grrt_last_error()
+            raise RuntimeError("grrt_create failed: " + (err.decode() if err else "unknown"))
+        if self.freqs is not None:
+            self._L.grrt_set_frequency_bins(self.ctx, _dptr(self.freqs), len(self.freqs))
+        self.width = vals.get("width", 0)
+        self.height = vals.get("height", 0)
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self._L.grrt_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            err = self._L.grrt_error(self.ctx)
+            raise RuntimeError(f"{what} failed: " + (err.decode() if err else f"rc={rc}"))
+
+    # --- reference API ---------------------------------------------------
+    def render(self) -> np.ndarray:
+        fb = np.empty((self.height, self.width, 4), dtype=np.float32)
+        self._check(self._L.grrt_render(self.ctx, fb.ctypes.data_as(C.POINTER(C.c_float))), "grrt_render")
+        return fb
+
+    def render_tile(self, x: int, y: int, w: int, h: int) -> np.ndarray:
+        fb = np.empty((h, w, 4), dtype=np.float32)
+        self._check(self._L.grrt_render_tile(self.ctx, fb.ctypes.data_as(C.POINTER(C.c_float)), x, y, w, h),
+                    "grrt_render_tile")
+        return fb
+
+    def render_spectral(self, width: Optional[int] = None, height: Optional[int] = None) -> np.ndarray:
+        w = width or self.width
+        h = height or self.height
+        nb = 0 if self.freqs is None else len(self.freqs)
+        out = np.empty((h, w, max(nb, 1)), dtype=np.float64)
+        self._check(self._L.grrt_render_spectral(self.ctx, _dptr(out), w, h), "grrt_render_spectral")
+        return out
+
+    def render_fits(self, path: str, width: Optional[int] = None, height: Optional[int] = None) -> None:
+        w = width or self.width
+        h = height or self.height
+        self._check(self._L.grrt_render_spectral_to_fits_cb(self.ctx, path.encode(), w, h, PROGRESS_FN(0), None),
+                    "grrt_render_spectral_to_fits_cb")
+
+    # --- additive API ----------------------------------------------------
+    def set_precision(self, form: int) -> None:
+        self._check(self._L.grrt_set_precision(self.ctx, form), "grrt_set_precision")
+
+    def set_mixed_params(self, r_factor: float, tol_fp32: float) -> None:
+        self._check(self._L.grrt_set_mixed_params(self.ctx, r_factor, tol_fp32), "grrt_set_mixed_params")
+
+    def render_device(self, d_rgba=None, d_rgb64=None, d_fate=None, stream=None) -> None:
+        """Render into device buffers given as raw pointers (int) or torch tensors."""
+        def ptr(x):
+            if x is None:
+                return None
+            return x if isinstance(x, int) else x.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_render_device(self.ctx, ptr(d_rgba), ptr(d_rgb64), ptr(d_fate), s),
+                    "grrt_render_device")
+
+    def render_spectral_device(self, d_spec, width: int, height: int, d_fate=None, stream=None) -> None:
+        def ptr(x):
+            if x is None:
+                return None
+            return x if isinstance(x, int) else x.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_render_spectral_device(self.ctx, ptr(d_spec), width, height, ptr(d_fate), s),
+                    "grrt_render_spectral_device")
+
+    def stats(self) -> dict:
+        st = GRRTStats()
+        self._check(self._L.grrt_get_stats(self.ctx, C.byref(st)), "grrt_get_stats")
+        return st.as_dict()
+
+    def table(self, name: str) -> np.ndarray:
+        n = self._L.grrt_scene_table(self.ctx, name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, dtype=np.float64)
+        self._L.grrt_scene_table(self.ctx, name.encode(), _dptr(out), n)
+        return out
+
+    def camera_ray(self, x: float, y: float) -> np.ndarray:
+        out = np.empty(8, dtype=np.float64)
+        self._L.grrt_camera_ray(self.ctx, x, y, _dptr(out))
+        return out
+
+
+def cuda_available() -> bool:
+    return bool(lib().grrt_cuda_available())

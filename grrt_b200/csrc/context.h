@@ -1,0 +1,88 @@
+// GRRTContext: resolved parameters, host tables, the device copy of the scene
+// and the per-context launch resources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/grrt_b200.h"
+#include "device/render_launch.h"
+#include "device/scene.h"
+#include "host/tables.h"
+
+struct GRRTContext {
+    GRRTParams params{};
+
+    // Resolved parameters (src/api.cpp:47-59, 72-75, 124, 141).
+    double mass = 1.0, spin_a = 0.0, observer_r = 50.0, observer_theta = 1.396, fov = 1.047;
+    double tolerance = 1e-8;
+    int max_steps = 10000, spp = 1;
+    double r_horizon = 2.0, isco = 6.0;
+
+    grrt_b200::CameraFrame cam{};
+    grrt_b200::SpectrumTable spectrum;
+    bool has_disk = false;
+    grrt_b200::FluxTable flux;
+    bool has_stars = false;
+    grrt_b200::StarCatalogue stars;
+    std::unique_ptr<grrt_b200::VolumetricTables> vol;
+    std::vector<double> ln_kabs;  // ln(max(kappa_abs, 1e-100)), precomputed for the device
+    std::vector<double> freq_bins;
+
+    // Precision form and its knobs.
+    int form = GRRT_FORM_FP64;
+    double mixed_r_factor = 3.0;
+    double tol_fp32 = 1e-6;
+
+    std::string error;
+    float progress = 0.0f;
+
+    // Device state (created at the first render).
+    int device = -1;
+    bool device_ready = false;
+    void* d_arena = nullptr;
+    grrt_b200::DevScene dev{};
+    unsigned int* d_queue = nullptr;
+    grrt_b200::DevStats* d_stats = nullptr;
+    int* h_cancel = nullptr;   // host-mapped
+    int* d_cancel = nullptr;   // its device alias
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_kernel_ms = 0.0;
+    // cached device outputs for the host-buffer entry points
+    void* d_out = nullptr;
+    size_t d_out_bytes = 0;
+    double* d_freqs = nullptr;
+    size_t d_freqs_n = 0;
+    double* d_spec_scratch = nullptr;
+    size_t d_spec_scratch_n = 0;
+
+    GRRTContext() = default;
+    ~GRRTContext();
+    GRRTContext(const GRRTContext&) = delete;
+    GRRTContext& operator=(const GRRTContext&) = delete;
+
+    void build(const GRRTParams& p);
+    bool ensure_device();
+    grrt_b200::DevScene scene_for_launch() const;
+
+    int render_rgb_device(const grrt_b200::DevTile& tile, float* d_rgba, double* d_rgb64, unsigned* d_fate,
+                          cudaStream_t s, bool reset_stats);
+    int render_rgb_to_host(const grrt_b200::DevTile& tile, float* host, grrt_progress_fn cb, void* user);
+    int render_spectral_device(int width, int height, double* d_spec, unsigned* d_fate, cudaStream_t s,
+                               bool reset_stats);
+    int render_spectral_to_host(int width, int height, double* host, grrt_progress_fn cb, void* user);
+    int render_spectral_to_fits(const char* path, int width, int height, grrt_progress_fn cb, void* user);
+    int read_stats(GRRTStats* out);
+    bool export_table(const std::string& name, std::vector<double>& out) const;
+    void debug_pixel(int px, int py);
+    void request_cancel();
+
+    // helpers
+    bool fail_cuda(cudaError_t e, const char* what);
+    void* scratch_output(size_t bytes);
+    int wait_with_progress(cudaStream_t s, unsigned total_pixels, grrt_progress_fn cb, void* user);
+};

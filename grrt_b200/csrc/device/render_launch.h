@@ -1,0 +1,47 @@
+// Host-side entry points of the render kernels (implemented in the .cu files).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "scene.h"
+
+namespace grrt_b200 {
+
+// Device outputs of an RGB launch; any pointer may be null.
+struct ThinOutputs {
+    float4* rgba = nullptr;     // linear HDR RGBA, tile.out_pitch pixels per row
+    double* rgb64 = nullptr;    // the spp-averaged double colour (3 per pixel)
+    uint32_t* fate = nullptr;   // per sample: termination | (disk crossings << 2)
+};
+
+// Device outputs of a spectral launch.
+struct SpectralOutputs {
+    double* spec = nullptr;     // [pixel][bin], pixel = qy*out_pitch + qx
+    uint32_t* fate = nullptr;
+};
+
+// Scratch a launch uses beside its inputs and outputs.
+struct LaunchResources {
+    unsigned int* queue = nullptr;    // work counter (zeroed by the launcher)
+    DevStats* stats = nullptr;        // accumulated counters
+    const volatile int* cancel = nullptr;  // host-mapped cancel flag, may be null
+    double* spectral_scratch = nullptr;    // spectral transfer state, see volume_spectral_scratch_elems
+    size_t spectral_scratch_elems = 0;
+};
+
+// Doubles of spectral scratch a launch with nb bins needs on the current device.
+size_t volume_spectral_scratch_elems(int nb);
+
+cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                        const LaunchResources& res, int form, cudaStream_t stream);
+
+cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                              const LaunchResources& res, int form, cudaStream_t stream);
+
+cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
+                                   const SpectralOutputs& out, const LaunchResources& res, int form,
+                                   cudaStream_t stream);
+
+}  // namespace grrt_b200

@@ -1,0 +1,114 @@
+// Device-side scene description shared by the host launcher and the kernels.
+//
+// One DevScene is passed by value to every render kernel (it lives in the
+// kernel parameter bank, so every field is a uniform, broadcast load). Tables
+// are device pointers into one arena allocated at grrt_create.
+#pragma once
+
+#include <cstdint>
+
+namespace grrt_b200 {
+
+enum : int { kTermHorizon = 0, kTermEscaped = 1, kTermMaxSteps = 2 };
+
+// Precision forms.
+enum : int { kFormFP64 = 0, kFormMixed = 1 };
+
+struct DevStars {
+    const double* theta = nullptr;
+    const double* phi = nullptr;
+    const double* brightness = nullptr;
+    const int* cell_start = nullptr;  // 180*360 + 1
+    const int* cell_items = nullptr;
+    double tol2 = 0.0;                // angular tolerance squared
+};
+
+struct DevVolume {
+    double M = 1, a = 0;  // the disk's own mass and spin (raw create parameters)
+    double r_min = 0, r_outer = 0, r_isco = 0, r_horizon = 0, taper_width = 0;
+    double E_isco = 0, L_isco = 0, rho_scale = 1, noise_scale = 1, turbulence = 0;
+    double inv_taper_w2 = 0;
+    int octaves = 2, n_r = 500, n_z = 128;
+    const double* H = nullptr;        // n_r
+    const double* z_max = nullptr;    // n_r
+    const double* rho_mid = nullptr;  // n_r
+    const double* rho_prof = nullptr; // n_r*n_z
+    const double* T_prof = nullptr;   // n_r*n_z
+    const int* perm = nullptr;        // 512
+    // opacity tables
+    int n_nu = 0, n_rho = 100, n_T = 100;
+    double log_nu_min = 0, log_nu_max = 0, log_rho_min = 0, log_rho_max = 0, log_T_min = 0, log_T_max = 0;
+    const double* ln_kabs = nullptr;  // ln(max(kappa_abs, 1e-100)), [n_nu][n_rho][n_T]
+    const double* kes = nullptr;      // [n_rho][n_T]
+    double ut_obs = 1;                // 1/sqrt(1 - 2/r_obs), the ray-march observer normalisation
+};
+
+struct DevScene {
+    // spacetime and integrator
+    double M = 1, a = 0;
+    double r_stop = 0;      // horizon radius + 0.01 (termination)
+    double r_escape = 1000; // escape radius
+    double tol = 1e-8;
+    double dl0 = 0.5;       // 0.01 * observer_r
+    double observer_r = 50;
+    int max_steps = 10000;
+
+    // camera
+    double cam_pos[4] = {0, 0, 0, 0};
+    double e0[4] = {0, 0, 0, 0}, e1[4] = {0, 0, 0, 0}, e2[4] = {0, 0, 0, 0}, e3[4] = {0, 0, 0, 0};
+    double g[16] = {};      // covariant metric at the camera, row-major
+    double fov = 1.047;
+    int width = 0, height = 0;
+    int grid = 1;           // floor(sqrt(spp))
+    double cell = 1.0;      // 1/grid
+    double inv_spp = 1.0;   // 1/grid^2
+
+    // thin disk
+    int disk_on = 0;
+    double r_in = 0, r_out = 0, flux_max = 0, peak_T = 0, u_t_obs = 1;
+    int flux_n = 0;
+    const double* flux = nullptr;
+
+    // blackbody chromaticity table
+    double t_min = 1000, t_max = 100000;
+    int spec_n = 0;
+    const double* spec_color = nullptr;  // 3*spec_n
+
+    int stars_on = 0;
+    DevStars stars;
+
+    int vol_on = 0;
+    DevVolume vol;
+
+    // mixed-precision form: outer steps starting at r > fp32_r_min use FP32
+    // right-hand sides, controlled against tol_fp32
+    double fp32_r_min = 0;
+    double tol_fp32 = 1e-6;
+};
+
+// Which pixels a launch covers: the rectangle [x0, x0+w) x [y0, y0+h) of the
+// image, written into an output of row pitch `out_pitch` pixels.
+struct DevTile {
+    int x0 = 0, y0 = 0, w = 0, h = 0;
+    int out_pitch = 0;
+};
+
+// Per-launch counters (summed over all threads with one atomic per warp).
+struct DevStats {
+    unsigned long long attempts;      // DP45 attempts
+    unsigned long long accepted;      // accepted outer steps
+    unsigned long long crossings;     // thin-disk emission events
+    unsigned long long rays;          // camera samples completed
+    unsigned long long horizon;       // terminations by kind
+    unsigned long long escaped;
+    unsigned long long max_steps;
+    unsigned long long clamp_evals;   // volumetric pre-step derivative evaluations
+    unsigned long long march_steps;   // volumetric RK4 steps
+    unsigned long long physics_steps; // volumetric steps with matter
+    unsigned long long bin_updates;   // per-frequency transfer updates
+    unsigned long long fp64_attempts; // mixed form: attempts taken in FP64
+    unsigned long long cancelled;     // launches that observed the cancel flag
+    unsigned long long pad[3];
+};
+
+}  // namespace grrt_b200

@@ -1,0 +1,267 @@
+// Thin-disk RGB render: camera -> Kerr null geodesic (adaptive DP45) ->
+// emission summed over every equatorial crossing inside [r_in, r_out] ->
+// first-match star lookup on escape. The per-pixel path of
+// GeodesicTracer::trace (src/geodesic_tracer.cpp:23-181) inside the loop of
+// Renderer::render (src/renderer.cpp:30-82), for both precision forms.
+//
+// Execution model: a persistent grid (resident blocks only). Each lane owns one
+// pixel at a time and walks its spp samples; each loop iteration performs
+// exactly one DP45 attempt for every lane with a live ray, so the warp stays
+// converged in the expensive part. A lane whose pixel is done takes the next
+// pixel from a global counter with one warp-aggregated atomic, which keeps
+// warps full while ray lengths range from tens to thousands of steps.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "integrate.cuh"
+#include "render_launch.h"
+#include "shading.cuh"
+
+namespace grrt_b200 {
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct LaneCounters {
+    unsigned long long attempts = 0, accepted = 0, crossings = 0, rays = 0;
+    unsigned long long horizon = 0, escaped = 0, maxsteps = 0, fp64_attempts = 0;
+};
+
+__device__ __forceinline__ void flush_counters(DevStats* st, const LaneCounters& c, bool cancelled) {
+    unsigned long long v[8] = {c.attempts, c.accepted, c.crossings, c.rays,
+                               c.horizon, c.escaped, c.maxsteps, c.fp64_attempts};
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(kFull, v[k], o);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&st->attempts, v[0]);
+        atomicAdd(&st->accepted, v[1]);
+        atomicAdd(&st->crossings, v[2]);
+        atomicAdd(&st->rays, v[3]);
+        atomicAdd(&st->horizon, v[4]);
+        atomicAdd(&st->escaped, v[5]);
+        atomicAdd(&st->max_steps, v[6]);
+        atomicAdd(&st->fp64_attempts, v[7]);
+        if (cancelled && threadIdx.x == 0) atomicAdd(&st->cancelled, 1ull);
+    }
+}
+
+// Start-of-step termination test in the reference order: step budget first
+// (the loop condition), then horizon, then escape.
+__device__ __forceinline__ int start_check(const DevScene& S, int step, double r) {
+    if (step >= S.max_steps) return kTermMaxSteps;
+    if (r < S.r_stop) return kTermHorizon;
+    if (r > S.r_escape) return kTermEscaped;
+    return -1;
+}
+
+}  // namespace
+
+template <int kForm>
+__global__ void __launch_bounds__(kThreads)
+thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
+                   double* __restrict__ out_rgb64, uint32_t* __restrict__ out_fate,
+                   unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
+                   const volatile int* __restrict__ cancel) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
+    const int grid2 = S.grid * S.grid;
+
+    LaneCounters cnt;
+    // pixel slot
+    int pix = -1;        // pixel index within the tile; -1 = needs a pixel; -2 = queue exhausted
+    int smp = 0;         // sample index within the pixel
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    // ray slot
+    bool live = false;
+    Vec5<double> y;      // state at the start of the current outer step
+    double pt = 0.0, pph = 0.0;
+    double dl = 0.0, dlambda = 0.0;
+    int retry = 0, step = 0, ncross = 0;
+    double col0 = 0.0, col1 = 0.0, col2 = 0.0;
+    bool cancelled = false;
+    unsigned iter = 0;
+
+    while (true) {
+        // ---- refill: lanes without a pixel take one (warp-aggregated atomic) ----
+        const bool want = (pix == -1);
+        const unsigned want_mask = __ballot_sync(kFull, want);
+        if (want_mask) {
+            unsigned base = 0;
+            const int leader = __ffs(want_mask) - 1;
+            if (lane == leader) base = atomicAdd(queue, static_cast<unsigned>(__popc(want_mask)));
+            base = __shfl_sync(kFull, base, leader);
+            if (want) {
+                const unsigned q = base + __popc(want_mask & lt_mask);
+                if (q < total) {
+                    pix = static_cast<int>(q);
+                    smp = 0;
+                    acc0 = acc1 = acc2 = 0.0;
+                } else {
+                    pix = -2;
+                }
+            }
+        }
+        // ---- start a ray for lanes that have a pixel but no live ray ----
+        if (!live && pix >= 0) {
+            const int qx = pix % tile.w, qy = pix / tile.w;
+            const int i = tile.x0 + qx, j = tile.y0 + qy;
+            const int sy = smp / S.grid, sx = smp % S.grid;
+            const double x = i + (sx + pixel_hash(i, j, smp, 0)) * S.cell;
+            const double yy = j + (sy + pixel_hash(i, j, smp, 1)) * S.cell;
+            double p[4];
+            camera_momentum(S, x, yy, p);
+            y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], p[1], p[2]};
+            pt = p[0];
+            pph = p[3];
+            dlambda = S.dl0;
+            dl = dlambda;
+            retry = 0;
+            step = 0;
+            ncross = 0;
+            col0 = col1 = col2 = 0.0;
+            live = true;
+        }
+        int term = -1;
+        if (live && retry == 0) term = start_check(S, step, y.r);
+
+        // ---- one DP45 attempt for every lane with a live, unterminated ray ----
+        if (live && term < 0) {
+            Vec5<double> y5;
+            double err;
+            double tol = S.tol;
+            if (kForm == kFormMixed && y.r > S.fp32_r_min) {
+                err = mixed_attempt_impl(static_cast<float>(S.M), static_cast<float>(S.a),
+                                         static_cast<float>(pt), static_cast<float>(pph), y, dl, y5);
+                tol = S.tol_fp32;
+            } else {
+                err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+                ++cnt.fp64_attempts;
+            }
+            ++cnt.attempts;
+            const StepDecision d = pi_control(err, tol, dl, retry, y5.r);
+            if (d.accept) {
+                ++cnt.accepted;
+                // equatorial crossing (src/geodesic_tracer.cpp:156-176): every
+                // crossing inside the disk adds emission; r is interpolated
+                // linearly in theta; p_t and p_phi are constants of motion.
+                if (S.disk_on) {
+                    const double d_prev = y.th - kHalfPi;
+                    const double d_new = y5.th - kHalfPi;
+                    if (d_prev * d_new < 0.0 && fabs(d_prev - d_new) > 1e-12) {
+                        const double frac = -d_prev / (d_new - d_prev);
+                        const double rc = y.r + frac * (y5.r - y.r);
+                        if (rc >= S.r_in && rc <= S.r_out) {
+                            double e0, e1, e2;
+                            disk_emission(S, rc, pt, pph, e0, e1, e2);
+                            col0 += e0;
+                            col1 += e1;
+                            col2 += e2;
+                            ++ncross;
+                            ++cnt.crossings;
+                        }
+                    }
+                }
+                y = y5;
+                dlambda = d.next;
+                dl = dlambda;
+                retry = 0;
+                ++step;
+                term = start_check(S, step, y.r);
+            } else {
+                dl = d.next;
+                ++retry;
+            }
+        }
+
+        // ---- finish a terminated sample ----
+        if (live && term >= 0) {
+            live = false;
+            ++cnt.rays;
+            if (term == kTermEscaped) {
+                ++cnt.escaped;
+                if (S.stars_on) {
+                    const double b = star_brightness(S.stars, y.th, y.ph);
+                    col0 += b;
+                    col1 += b;
+                    col2 += b;
+                }
+            } else if (term == kTermHorizon) {
+                ++cnt.horizon;
+            } else {
+                ++cnt.maxsteps;
+            }
+            acc0 = acc0 + col0;
+            acc1 = acc1 + col1;
+            acc2 = acc2 + col2;
+            if (out_fate) {
+                const unsigned nc = (ncross > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(ncross);
+                out_fate[static_cast<size_t>(pix) * grid2 + smp] = static_cast<unsigned>(term) | (nc << 2);
+            }
+            if (++smp == grid2) {
+                const int qx = pix % tile.w, qy = pix / tile.w;
+                const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
+                const double r0 = acc0 * S.inv_spp, r1 = acc1 * S.inv_spp, r2 = acc2 * S.inv_spp;
+                if (out_rgba) out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1),
+                                                         static_cast<float>(r2), 1.0f);
+                if (out_rgb64) {
+                    out_rgb64[3 * o + 0] = r0;
+                    out_rgb64[3 * o + 1] = r1;
+                    out_rgb64[3 * o + 2] = r2;
+                }
+                pix = -1;
+            }
+        }
+
+        // ---- cancellation (host-mapped flag, polled by one lane per warp) ----
+        if (cancel && ((++iter & 1023u) == 0)) {
+            int c = 0;
+            if (lane == 0) c = *cancel;
+            c = __shfl_sync(kFull, c, 0);
+            if (c) {
+                cancelled = true;
+                break;
+            }
+        }
+        // ---- exit when the queue is drained and no lane holds a ray ----
+        if (!__any_sync(kFull, live || pix >= -1)) break;
+    }
+    flush_counters(stats, cnt, cancelled);
+}
+
+template <int kForm>
+static cudaError_t launch_thin_form(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                                    const LaunchResources& res, cudaStream_t stream) {
+    static int blocks_per_sm = 0;
+    static int num_sms = 0;
+    if (blocks_per_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, thin_render_kernel<kForm>, kThreads, 0);
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+    }
+    const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
+    if (total == 0) return cudaSuccess;
+    int blocks = num_sms * blocks_per_sm;
+    const int needed = static_cast<int>((total + kThreads - 1) / kThreads);
+    if (needed < blocks) blocks = needed;
+    cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+    thin_render_kernel<kForm><<<blocks, kThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate,
+                                                               res.queue, res.stats, res.cancel);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                        const LaunchResources& res, int form, cudaStream_t stream) {
+    if (form == kFormMixed) return launch_thin_form<kFormMixed>(S, tile, out, res, stream);
+    return launch_thin_form<kFormFP64>(S, tile, out, res, stream);
+}
+
+}  // namespace grrt_b200

@@ -1,0 +1,153 @@
+"""Device renders (plain FP64 form) against the oracle, through the C ABI.
+
+Bar of the FP64 form:
+  * fate (termination and number of emitting disk crossings, or ray-march
+    entries) equals the oracle's for every sample outside the fate band;
+  * outside the rounding-sensitive band (tests/parity_util.py), at least
+    MIN_WITHIN of the pixels are within TOL = 1e-9 relative of the oracle's
+    double intensity and every pixel is within LOOSE = 1e-6 (an error there
+    is a bug, not rounding);
+  * the band stays below the stated fraction.
+The band is probed, not exhaustive: a pixel whose own rounding noise straddles
+1e-9 can escape the probes, which is why the 1e-9 bar is stated as a fraction.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from parity_util import OracleRGB, OracleSpectral, device_render_rgb, device_render_spectral, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-9
+LOOSE = 1e-6
+MIN_WITHIN = 0.995
+MAX_BAND = 0.06  # fraction of pixels allowed in the rounding-sensitive band (1 spp)
+
+
+def check_rgb(grrt, R, pix_all: bool = True, n_sample: int = 0, seed: int = 0, max_band=MAX_BAND):
+    W, H = R.width, R.height
+    spp = R.values.get("samples_per_pixel", 1)
+    rgba, rgb64, fate, stats = device_render_rgb(R, spp)
+    g2 = max(1, int(math.sqrt(spp))) ** 2
+    # counters are consistent with the image
+    assert stats["rays"] == W * H * g2
+    assert stats["horizon"] + stats["escaped"] + stats["max_steps"] == stats["rays"]
+    assert stats["attempts"] >= stats["accepted"] > 0
+    # the float framebuffer is the float cast of the double mean, alpha 1
+    np.testing.assert_array_equal(rgba[..., :3], rgb64.astype(np.float32))
+    assert np.all(rgba[..., 3] == 1.0)
+    if pix_all:
+        pix = np.arange(W * H)
+    else:
+        pix = np.random.default_rng(seed).choice(W * H, size=n_sample, replace=False)
+    orc = OracleRGB(R, pix, TOL)
+    got = rgb64.reshape(-1, 3)[pix]
+    gfate = fate.reshape(-1, g2)[pix].ravel()
+    band = orc.pixel_band
+    frac = band.mean()
+    assert frac <= max_band, f"rounding-sensitive band {frac:.4f} of pixels"
+    fate_out = ~np.repeat(orc.pixel_fate_band, g2)
+    mism = np.nonzero(fate_out & (gfate != orc.fate))[0]
+    assert len(mism) == 0, f"{len(mism)} fate mismatches outside the fate band, e.g. sample {mism[:5]}"
+    err = np.max(rel_err(got, orc.pixel_rgb, floor=1e-300), axis=1)
+    out = ~band
+    within = float(np.mean(err[out] <= TOL)) if out.any() else 1.0
+    worst = float(np.max(err[out])) if out.any() else 0.0
+    assert within >= MIN_WITHIN, f"only {within:.4%} of pixels outside the band within {TOL}"
+    assert worst <= LOOSE, f"max relative error outside the band {worst:.3e}"
+    # work: same method, so the attempt count matches the oracle's closely
+    if pix_all:
+        assert abs(stats["attempts"] - orc.counters["attempts"]) <= 0.01 * orc.counters["attempts"]
+        assert stats["crossings"] == orc.counters["crossings"] or frac > 0
+    return frac, worst, stats, orc
+
+
+def test_schwarzschild_thin_256_full_image(grrt, need_gpu):
+    R = grrt.Renderer(grrt.config_params(1))  # 256x256, 1 spp, black background
+    frac, worst, stats, orc = check_rgb(grrt, R)
+    assert (orc.term == 0).any() and (orc.ncross > 0).any()
+    print(f"\nC1 256^2: band {frac:.4%}, worst rel err outside band {worst:.2e}, attempts {stats['attempts']}")
+
+
+def test_kerr_thin_stars_4spp(grrt, need_gpu):
+    R = grrt.Renderer(grrt.config_params(2, width=160, height=160))  # 4 spp, stars
+    frac, worst, stats, orc = check_rgb(grrt, R, max_band=0.15)
+    assert (orc.ncross > 1).any(), "higher-order images expected"
+    print(f"\nC2 160^2x4: band {frac:.4%}, worst {worst:.2e}")
+
+
+def test_kerr_thin_full_size_sampled(grrt, need_gpu):
+    """The 1024^2 4-spp scene at full size; parity on a random pixel subset."""
+    R = grrt.Renderer(grrt.config_params(2))
+    frac, worst, stats, orc = check_rgb(grrt, R, pix_all=False, n_sample=1500, seed=5, max_band=0.15)
+    assert stats["rays"] == 1024 * 1024 * 4
+    print(f"\nC2 1024^2x4 sampled: band {frac:.4%}, worst {worst:.2e}, attempts/ray "
+          f"{stats['attempts'] / stats['rays']:.1f}")
+
+
+@pytest.mark.parametrize("variant", [
+    dict(spin=0.5, observer_theta=math.radians(30.0)),
+    dict(spin=0.9, observer_theta=math.radians(89.0), observer_phi=1.0, disk_inner=8.0, disk_outer=30.0),
+    dict(metric_type=0, observer_r=20.0, fov=math.radians(40.0), samples_per_pixel=9),
+])
+def test_thin_variants(grrt, need_gpu, variant):
+    vals = grrt.config_params(2, width=64, height=48, **variant)
+    R = grrt.Renderer(vals)
+    check_rgb(grrt, R, max_band=0.3)
+
+
+def test_volumetric_rgb(grrt, need_gpu):
+    freqs = grrt.log_bins(1e14, 1e18, 32)
+    R = grrt.Renderer(grrt.config_params(3, width=64, height=64), freqs=freqs)
+    frac, worst, stats, orc = check_rgb(grrt, R, max_band=0.3)
+    assert stats["march_steps"] > 0 and stats["physics_steps"] > 0
+    assert stats["march_steps"] == orc.counters["march_steps"] or frac > 0
+    print(f"\nC3 RGB 64^2: band {frac:.4%}, worst {worst:.2e}")
+
+
+def check_spectral(grrt, R, freqs, pix, max_band):
+    nb = len(freqs)
+    spec, fate, stats = device_render_spectral(R, nb)
+    W, H = R.width, R.height
+    orc = OracleSpectral(R, freqs, pix, TOL)
+    got = spec.reshape(-1, nb)[pix]
+    band = orc.pixel_band
+    frac = band.mean()
+    assert frac <= max_band, f"band {frac:.3f}"
+    g2 = orc.g2
+    gterm = (fate.reshape(-1, g2)[pix].ravel() & 3).astype(np.int32)
+    fate_out = ~np.repeat(orc.pixel_fate_band, g2)
+    assert np.all(gterm[fate_out] == orc.term[fate_out])
+    err = np.max(rel_err(got, orc.pixel_spec), axis=1)
+    out = ~band
+    within = float(np.mean(err[out] <= TOL)) if out.any() else 1.0
+    worst = float(np.max(err[out])) if out.any() else 0.0
+    assert within >= MIN_WITHIN, f"only {within:.4%} of pixels outside the band within {TOL}"
+    assert worst <= LOOSE, f"max relative error outside the band {worst:.3e}"
+    assert stats["bin_updates"] == stats["physics_steps"] * nb
+    return frac, worst, stats
+
+
+def test_volumetric_spectral(grrt, need_gpu):
+    freqs = grrt.log_bins(1e14, 1e18, 32)
+    R = grrt.Renderer(grrt.config_params(3, width=64, height=64), freqs=freqs)
+    frac, worst, stats = check_spectral(grrt, R, freqs, np.arange(64 * 64), max_band=0.3)
+    print(f"\nC3 spectral 64^2x32: band {frac:.4%}, worst {worst:.2e}, physics steps {stats['physics_steps']}")
+
+
+def test_volumetric_spectral_full_size_sampled(grrt, need_gpu):
+    freqs = grrt.log_bins(1e14, 1e18, 32)
+    R = grrt.Renderer(grrt.config_params(3), freqs=freqs)  # 512^2
+    pix = np.random.default_rng(9).choice(512 * 512, size=600, replace=False)
+    frac, worst, stats = check_spectral(grrt, R, freqs, pix, max_band=0.3)
+    assert stats["rays"] == 512 * 512
+
+
+def test_no_volumetric_disk_gives_zero_spectra(grrt, need_gpu):
+    """trace_spectral returns zeros without a volumetric disk (src/geodesic_tracer.cpp:503-505)."""
+    freqs = grrt.log_bins(1e14, 1e18, 4)
+    R = grrt.Renderer(grrt.config_params(2, width=32, height=16), freqs=freqs)
+    out = R.render_spectral()
+    assert out.shape == (16, 32, 4) and np.all(out == 0.0)
