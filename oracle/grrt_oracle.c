@@ -741,6 +741,7 @@ static int trace_one(const OracleScene* sc, const double* init, double* rgb, int
                 memcpy(entry, prev, sizeof entry);
                 march_rgb(sc, entry, J, T, cnt);
                 memcpy(y, entry, sizeof y);
+                ++nc;  /* with a volumetric disk the fate counts ray-march entries */
                 continue;
             }
         }

@@ -71,8 +71,9 @@ void oracle_camera_ray(const OracleScene* sc, double x, double y, double* out);
 
 /* Trace n camera samples at fractional pixel coordinates (GeodesicTracer::trace
  * plus the star lookup of Renderer::render). rgb[3n], term[n] (0 horizon,
- * 1 escaped, 2 max steps), ncross[n] emitting disk crossings, fin[8n] final
- * state (may be NULL). OpenMP over samples. */
+ * 1 escaped, 2 max steps), ncross[n] emitting disk crossings (with a
+ * volumetric disk: ray-march entries), fin[8n] final state (may be NULL).
+ * OpenMP over samples. */
 void oracle_trace_rgb(const OracleScene* sc, int n, const double* px, const double* py,
                       double* rgb, int* term, int* ncross, double* fin, OracleCounters* cnt);
 
