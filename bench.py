@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # smaller frames of the same scene, for profiler captures (default: the benchmark frame)
+    ap.add_argument("--width", type=int, default=1024)
+    ap.add_argument("--height", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -153,10 +156,10 @@ def cpu_reference_sample(row_offset: int = 0, stride: int = 16):
     import grrt_b200 as G
     import oracle_bind
     kind = "fast" if oracle_bind.ref_available("fast") else "strict"
-    ref = oracle_bind.RefScene(G.config_params(2), kind=kind)
+    ref = oracle_bind.RefScene(G.config_params(2), kind=kind)  # the 1024x1024 benchmark frame
     _, secs, threads = ref.render_rows(row_offset, stride)
-    rows = len(range(row_offset, H, stride))
-    rays = rows * W * SPP
+    rows = len(range(row_offset, 1024, stride))
+    rays = rows * 1024 * SPP
     return rays, secs, threads, kind, rows
 
 
@@ -173,7 +176,7 @@ def run_reference_arm(args):
         total_rays += rays
         total_secs += secs
     value = total_rays / total_secs
-    sample = (f"every {stride}th row of the 1024x1024 4-spp frame ({rows} rows, {rows * W * SPP} rays) per step, "
+    sample = (f"every {stride}th row of the 1024x1024 4-spp frame ({rows} rows, {rows * 1024 * SPP} rays) per step, "
               f"row offset = step mod {stride}; reference src/*.cpp built with its shipped flags "
               f"(minus -march=native and LTO), OpenMP over all host threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": args.gpus,
@@ -190,7 +193,12 @@ def run_reference_arm(args):
 # our arm
 # ---------------------------------------------------------------------------
 def main():
+    global W, H, RAYS, WORKLOAD
     args = parse()
+    if (args.width, args.height) != (W, H):
+        W, H = args.width, args.height
+        RAYS = W * H * SPP
+        WORKLOAD = WORKLOAD.replace("1024x1024", f"{W}x{H}")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -207,7 +215,7 @@ def main():
     import grrt_b200 as G
 
     form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
-    R = G.Renderer(G.config_params(2))
+    R = G.Renderer(G.config_params(2, width=W, height=H))
     R.set_precision(form)
     stream = torch.cuda.Stream()
     rgba = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
@@ -293,7 +301,7 @@ def main():
             try:
                 rays, secs, threads, kind, rows = cpu_reference_sample(0, 16)
                 cpu = {"value": rays / secs, "unit": "rays/s", "cores": threads, "kind": "reference",
-                       "sample": f"rows 0,16,...,1008 of the same frame ({rows * W * SPP} rays), reference "
+                       "sample": f"rows 0,16,...,1008 of the 1024x1024 4-spp frame ({rays} rays), reference "
                                  f"src/*.cpp ({kind} build) via oracle/_ref, OpenMP, {secs:.2f} s"}
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "unit": "rays/s", "cores": os.cpu_count(), "kind": "reference",
