@@ -118,6 +118,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_set_mixed_params": (C.c_int, [vp, C.c_double, C.c_double]),
         "grrt_render_device": (C.c_int, [vp, vp, vp, vp, vp]),
         "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
+        "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
         "grrt_scene_table": (C.c_longlong, [vp, C.c_char_p, P(C.c_double), C.c_longlong]),
         "grrt_camera_ray": (C.c_int, [vp, C.c_double, C.c_double, P(C.c_double)]),
@@ -285,6 +286,15 @@ class Renderer:
         s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
         self._check(self._L.grrt_render_spectral_device(self.ctx, ptr(d_spec), width, height, ptr(d_fate), s),
                     "grrt_render_spectral_device")
+
+    def render_spectral_device_noalloc(self, d_freqs, nb: int, d_spec, width: int, height: int,
+                                       stream=None) -> None:
+        """The spectral render that allocates no device memory (fixed in-library scratch)."""
+        fp = d_freqs if isinstance(d_freqs, int) else d_freqs.data_ptr()
+        sp = d_spec if isinstance(d_spec, int) else d_spec.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_render_spectral_device_noalloc(self.ctx, fp, nb, sp, width, height, s),
+                    "grrt_render_spectral_device_noalloc")
 
     def stats(self) -> dict:
         st = GRRTStats()

@@ -44,4 +44,11 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
                                    const SpectralOutputs& out, const LaunchResources& res, int form,
                                    cudaStream_t stream);
 
+// Spectral render whose scratch is a file-scope device array (no allocation);
+// see vol_render.cu. Returns cudaErrorInvalidValue when nb exceeds the limit.
+cudaError_t launch_volume_spectral_noalloc(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
+                                           double* out_spec, int form, cudaStream_t stream);
+int volume_spectral_noalloc_max_bins();
+size_t volume_spectral_noalloc_bytes();
+
 }  // namespace grrt_b200

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "integrate.cuh"
 #include "render_launch.h"
@@ -442,6 +443,80 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
     if (form == kFormMixed)
         return launch_vol<true, kFormMixed>(S, tile, freqs, nb, nullptr, out.spec, out.fate, res, stream);
     return launch_vol<true, kFormFP64>(S, tile, freqs, nb, nullptr, out.spec, out.fate, res, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Spectral render without any device allocation.
+//
+// For callers that must not allocate device memory while they render: a host
+// application that hands the renderer a fixed memory budget and forbids
+// driver allocations during a frame, a pipeline recorded into a CUDA graph
+// (cudaMalloc cannot be captured), or a process running near the device
+// memory limit where an allocation could fail mid-frame. The per-launch
+// scratch (work counter, counters, and the per-lane J, T, tau and pixel-sum
+// transfer state) lives in the file-scope array below instead of cudaMalloc'd
+// memory. Every GPU that loads the library holds this array until the process
+// exits.
+//
+// Limits: at most kNoAllocMaxBins frequency bins, one fixed grid of
+// kNoAllocBlocks x kVolThreads lanes. All calls share the one array, which
+// keeps the last call's contents; launches of this entry point that overlap on
+// the GPU (two streams, or two threads) race on it and must be serialised by
+// the caller.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocMaxBins = 32;
+constexpr int kNoAllocBlocks = 148;  // one block per B200 SM
+constexpr size_t kNoAllocSlots = static_cast<size_t>(kNoAllocBlocks) * kVolThreads;
+constexpr size_t kNoAllocHeader = 512;  // [0,256): work counter, [256,512): DevStats
+constexpr size_t kNoAllocBytes = kNoAllocHeader + sizeof(double) * 4 * kNoAllocMaxBins * kNoAllocSlots;
+static_assert(sizeof(DevStats) <= 256, "stats must fit the header");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+}  // namespace
+
+int volume_spectral_noalloc_max_bins() { return kNoAllocMaxBins; }
+size_t volume_spectral_noalloc_bytes() { return kNoAllocBytes; }
+
+cudaError_t launch_volume_spectral_noalloc(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
+                                           double* out_spec, int form, cudaStream_t stream) {
+    if (nb < 1 || nb > kNoAllocMaxBins) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    unsigned char* base = nullptr;
+    {
+        // Set-up, once per device with that device current: the host-side name
+        // of the array is not a device address, so ask the runtime for it.
+        std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return e;
+            g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
+    if (total == 0) return cudaSuccess;
+    // The work counter must start at zero; the counters are cleared with it.
+    e = cudaMemsetAsync(base, 0, kNoAllocHeader, stream);
+    if (e != cudaSuccess) return e;
+    auto* queue = reinterpret_cast<unsigned int*>(base);
+    auto* stats = reinterpret_cast<DevStats*>(base + 256);
+    auto* transfer = reinterpret_cast<double*>(base + kNoAllocHeader);
+    if (form == kFormMixed)
+        vol_render_kernel<true, kFormMixed><<<kNoAllocBlocks, kVolThreads, 0, stream>>>(
+            S, tile, freqs, nb, nullptr, out_spec, nullptr, transfer, queue, stats, nullptr);
+    else
+        vol_render_kernel<true, kFormFP64><<<kNoAllocBlocks, kVolThreads, 0, stream>>>(
+            S, tile, freqs, nb, nullptr, out_spec, nullptr, transfer, queue, stats, nullptr);
+    return cudaGetLastError();
 }
 
 }  // namespace grrt_b200

@@ -65,6 +65,30 @@ GRRT_EXPORT int grrt_render_device(GRRTContext* ctx, float* d_rgba, double* d_rg
 GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double* d_spec, int width, int height,
                                             unsigned int* d_fate, void* stream);
 
+/* Spectral render that allocates no device memory. No counterpart in the
+ * reference (its renders run on host threads and allocate host buffers).
+ *
+ * For callers that may not allocate device memory while they render: a host
+ * application that gives the renderer a fixed memory budget and forbids
+ * driver allocations during a frame, work recorded into a CUDA graph
+ * (cudaMalloc cannot be captured), or a process near the device memory limit
+ * where an allocation could fail mid-frame. Instead of cudaMalloc'd scratch it
+ * uses a fixed array compiled into the library (about 19.4 MB on every GPU that
+ * loads it, held until the process exits). The caller passes the inputs and
+ * outputs: d_freqs (num_bins observer-frame frequencies in Hz, device memory)
+ * and d_spec (double[width*height*num_bins], device memory); the scene comes
+ * from the context, which must already hold it on the device (any earlier
+ * render call on the context uploads it). Same output as
+ * grrt_render_spectral_device, enqueued on `stream`.
+ *
+ * Limits: num_bins <= 32, otherwise -1 with grrt_error set. The first call on
+ * each device looks up the array's device address; make that first call before
+ * any stream capture. All calls share the array and it keeps the last call's
+ * contents, so calls that overlap on the GPU race and must be serialised by
+ * the caller. It does not update grrt_get_stats and does not poll grrt_cancel. */
+GRRT_EXPORT int grrt_render_spectral_device_noalloc(GRRTContext* ctx, const double* d_freqs, int num_bins,
+                                                    double* d_spec, int width, int height, void* stream);
+
 /* Counters of the last render; synchronises the context's device. */
 GRRT_EXPORT int grrt_get_stats(GRRTContext* ctx, GRRTStats* out);
 
