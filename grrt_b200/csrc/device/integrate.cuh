@@ -29,13 +29,13 @@ constexpr double e1 = 71.0 / 57600.0, e3 = -71.0 / 16695.0, e4 = 71.0 / 1920.0,
 }  // namespace dp
 
 template <typename T>
-__device__ __forceinline__ Vec5<T> axpy(const Vec5<T>& y, T h, const Vec5<T>& k) {
+GRRT_HD Vec5<T> axpy(const Vec5<T>& y, T h, const Vec5<T>& k) {
     return Vec5<T>{y.r + h * k.r, y.th + h * k.th, y.ph + h * k.ph, y.pr + h * k.pr, y.pth + h * k.pth};
 }
 
 // Classic RK4 step (include/grrt/geodesic/rk4.h:34-52).
 template <typename T>
-__device__ __forceinline__ Vec5<T> rk4_step(T M, T a, T pt, T pph, const Vec5<T>& y, T h) {
+GRRT_HD Vec5<T> rk4_step(T M, T a, T pt, T pph, const Vec5<T>& y, T h) {
     const Vec5<T> k1 = kerr_rhs<T>(M, a, pt, pph, y);
     const Vec5<T> k2 = kerr_rhs<T>(M, a, pt, pph, axpy(y, h * T(0.5), k1));
     const Vec5<T> k3 = kerr_rhs<T>(M, a, pt, pph, axpy(y, h * T(0.5), k2));
@@ -48,7 +48,7 @@ __device__ __forceinline__ Vec5<T> rk4_step(T M, T a, T pt, T pph, const Vec5<T>
 
 // One DP45 attempt: returns the 5th-order state in y5 and the error norm.
 template <typename T>
-__device__ __forceinline__ T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5) {
+GRRT_HD T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5) {
     using namespace dp;
     const Vec5<T> k1 = kerr_rhs<T>(M, a, pt, pph, y);
 #define GRRT_S2(f) y.f + h * (T(a21) * k1.f)
@@ -131,7 +131,7 @@ __device__ __forceinline__ double mixed_attempt_impl(float M, float a, float pt,
     float err = 0.0f;
 #define GRRT_ERRF(f)                                                                     \
     {                                                                                    \
-        const float v = fabsf(h * (e.f + float(e7) * k7.f)) / (fabsf(y5f.f) + 1e-10f); \
+        const float v = fabsf(h * (e.f + float(e7) * k7.f)) * recip(fabsf(y5f.f) + 1e-10f); \
         err = (err < v) ? v : err;                                                       \
     }
     GRRT_ERRF(r) GRRT_ERRF(th) GRRT_ERRF(ph) GRRT_ERRF(pr) GRRT_ERRF(pth)

@@ -1,19 +1,34 @@
 // Kerr null-geodesic right-hand side in Boyer-Lindquist coordinates, for the
-// Hamiltonian form H = 1/2 g^{mu nu} p_mu p_nu with covariant momenta.
+// Hamiltonian H = 1/2 g^{mu nu} p_mu p_nu with covariant momenta: the same
+// equations as Kerr::compute_derivatives_inline
+// (include/grrt/spacetime/kerr.h:31-109), with the same pole clamp of sin(theta)
+// and the same Cody-Waite/Cephes sin-cos (include/grrt/math/fast_trig.h:21-82).
 //
-// Follows Kerr::compute_derivatives_inline (include/grrt/spacetime/kerr.h:31-109):
-// same metric, same analytic derivatives, same pole clamp and the same
-// Cody-Waite/Cephes sin-cos (include/grrt/math/fast_trig.h:21-82). The algebra
-// is rearranged for the GPU: the (t,phi) block inverse and the r/theta terms
-// share 1/Sigma and 1/det, and 1/Delta cancels against dx^r = Delta p_r / Sigma,
-// so one evaluation needs two divisions instead of seventeen. The result equals
-// the reference expression up to rounding (a few ulp per evaluation).
+// The Kerr inverse metric separates (Carter): with
+//     P(r) = (r^2 + a^2) p_t + a p_phi,   Q(theta) = a sin(theta) p_t + p_phi / sin(theta),
+//     2 Sigma H = F(r) + G(theta),  F = Delta p_r^2 - P^2 / Delta,  G = p_theta^2 + Q^2,
+// so dx/dlambda = dH/dp and dp/dlambda = -dH/dx follow from F, G and their
+// derivatives with one division (1/(Sigma Delta sin)) instead of the
+// reference's seventeen. The value is the reference's function; the rounding
+// differs by a few ulp per evaluation. The identity is checked against the
+// reference form on the CPU (tests/test_device_math.py).
 //
 // State layout: r, theta, phi, p_r, p_theta; p_t and p_phi are constants of
 // motion (dp_t = dp_phi = 0) and t does not feed back, so neither is integrated.
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <cmath>
+
+#define GRRT_HD __host__ __device__ __forceinline__
+// The right-hand side is inlined at its seven call sites per attempt unless
+// GRRT_RHS_CALL is set (one shared body: less code, a call per evaluation).
+#ifdef GRRT_RHS_CALL
+#define GRRT_RHS_ATTR __host__ __device__ __noinline__
+#else
+#define GRRT_RHS_ATTR GRRT_HD
+#endif
 
 namespace grrt_b200 {
 
@@ -24,7 +39,7 @@ struct Vec5 {
 
 // Cody-Waite reduction to [-pi/4, pi/4], then the degree-11/10 Cephes
 // polynomials (public-domain coefficients, S. Moshier), as fast_trig.h:21-82.
-__device__ __forceinline__ void fast_sincos(double x, double& s, double& c) {
+GRRT_HD void fast_sincos(double x, double& s, double& c) {
     constexpr double DP1 = 7.85398125648498535156e-1, DP2 = 3.77489470793079817668e-8,
                      DP3 = 2.69515142907905952645e-15, FOPI = 1.27323954473516268615;
     constexpr double S0 = -1.66666666666666324348e-01, S1 = 8.33333333332248946124e-03,
@@ -55,53 +70,78 @@ __device__ __forceinline__ void fast_sincos(double x, double& s, double& c) {
     c = flip_c ? -cv : cv;
 }
 
-// FP32 counterpart for the mixed form: CUDA's single-precision sincosf
-// (full range reduction, a few ulp).
-__device__ __forceinline__ void fast_sincos(float x, float& s, float& c) { sincosf(x, &s, &c); }
+// FP32 counterpart for the mixed form: the same octant reduction with a
+// three-part float pi/4 and the Cephes single-precision polynomials
+// (public-domain coefficients, S. Moshier), accurate to a few float ulp for the
+// |theta| < 1e4 the integrator can reach.
+GRRT_HD void fast_sincos(float x, float& s, float& c) {
+    constexpr float DP1 = 0.78515625f, DP2 = 2.4187564849853515625e-4f, DP3 = 3.77489497744594108e-8f;
+    constexpr float FOPI = 1.27323954473516f;
+    float ax = fabsf(x);
+    const bool neg = x < 0.0f;
+    int j = static_cast<int>(ax * FOPI);
+    j = (j + 1) & ~1;
+    const float y = static_cast<float>(j);
+    ax = ((ax - y * DP1) - y * DP2) - y * DP3;
+    int oct = j & 7;
+    bool flip_s = neg, flip_c = false;
+    if (oct > 3) { flip_s = !flip_s; flip_c = !flip_c; oct -= 4; }
+    if (oct > 1) flip_c = !flip_c;
+    const float z = ax * ax;
+    const float sr = ((-1.9515295891e-4f * z + 8.3321608736e-3f) * z - 1.6666654611e-1f) * z * ax + ax;
+    const float cr = ((2.443315711809948e-5f * z - 1.388731625493765e-3f) * z + 4.166664568298827e-2f) * z * z
+                     - 0.5f * z + 1.0f;
+    const bool swap = (oct == 1 || oct == 2);
+    const float sv = swap ? cr : sr;
+    const float cv = swap ? sr : cr;
+    s = flip_s ? -sv : sv;
+    c = flip_c ? -cv : cv;
+}
+
+// 1/x: IEEE division in FP64; in FP32 the hardware reciprocal approximation
+// (about 1 ulp), which the FP32 form's error budget absorbs.
+GRRT_HD double recip(double x) { return 1.0 / x; }
+GRRT_HD float recip(float x) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(1.0f, x);
+#else
+    return 1.0f / x;
+#endif
+}
 
 // Returns dx/dlambda and dp/dlambda for (r, theta, phi, p_r, p_theta) given the
 // constants p_t, p_phi.
 template <typename T>
-__device__ __forceinline__ Vec5<T> kerr_rhs(T M, T a, T pt, T pph, const Vec5<T>& y) {
-    const T r = y.r;
+GRRT_RHS_ATTR Vec5<T> kerr_rhs(T M, T a, T pt, T pph, const Vec5<T>& y) {
+    using std::fabs;
+    const T r = y.r, pr = y.pr, pth = y.pth;
     T s, c;
     fast_sincos(y.th, s, c);
     if (fabs(s) < T(1e-10)) s = (s >= T(0)) ? T(1e-10) : T(-1e-10);
     const T r2 = r * r, a2 = a * a;
-    const T s2 = s * s, c2 = c * c;
-    const T s2t = T(2) * s * c;
-    const T Mr = M * r;
-    const T Sigma = r2 + a2 * c2;
-    const T Delta = r2 - T(2) * Mr + a2;
-    const T iS = T(1) / Sigma;
-    const T iS2 = iS * iS;
-    // covariant (t, phi) block
-    const T two_Mr_iS = T(2) * Mr * iS;
-    const T g_tt = two_Mr_iS - T(1);
-    const T g_tphi = -two_Mr_iS * a * s2;
-    const T g_phph = (r2 + a2 + two_Mr_iS * a2 * s2) * s2;
-    const T idet = T(1) / (g_tt * g_phph - g_tphi * g_tphi);
-    // dx^mu = g^{mu nu} p_nu
-    const T dt = (g_phph * pt - g_tphi * pph) * idet;
-    const T dph = (g_tt * pph - g_tphi * pt) * idet;
-    const T dr = Delta * iS * y.pr;
-    const T dth = iS * y.pth;
-    // -dH/dr
-    const T Sm = Sigma - T(2) * r2;
-    const T dgtt_r = T(2) * M * Sm * iS2;
-    const T dgtp_r = -a * s2 * dgtt_r;
-    const T dgpp_r = T(2) * r * s2 + a2 * s2 * s2 * dgtt_r;
-    const T grr_r_pr2 = (T(2) * r * Delta - T(2) * Sigma * (r - M)) * iS2 * y.pr * y.pr;
-    const T dp_r = T(0.5) * (dgtt_r * dt * dt + T(2) * dgtp_r * dt * dph + grr_r_pr2
-                             + T(2) * r * dth * dth + dgpp_r * dph * dph);
-    // -dH/dtheta
-    const T k = T(2) * Mr * a2 * s2t * iS2;  // d g_tt / d theta
-    const T dgtp_th = -T(2) * Mr * a * s2t * (Sigma + a2 * s2) * iS2;
-    const T grr_th_pr2 = -a2 * s2t * Delta * iS2 * y.pr * y.pr;
-    const T dgpp_th = (r2 + a2) * s2t + k * s2 * (T(2) * Sigma + a2 * s2);
-    const T dp_th = T(0.5) * (k * dt * dt + T(2) * dgtp_th * dt * dph + grr_th_pr2
-                              - a2 * s2t * dth * dth + dgpp_th * dph * dph);
-    return Vec5<T>{dr, dth, dph, dp_r, dp_th};
+    const T Sigma = r2 + a2 * c * c;
+    const T Delta = r2 - T(2) * M * r + a2;
+    const T SD = Sigma * Delta;
+    const T inv = recip(SD * s);
+    const T iS = Delta * s * inv;  // 1/Sigma
+    const T iD = Sigma * s * inv;  // 1/Delta
+    const T is = SD * inv;         // 1/sin(theta)
+    const T P = (r2 + a2) * pt + a * pph;
+    const T Q = a * s * pt + pph * is;
+    const T PiD = P * iD;
+    const T hiS = T(0.5) * iS;
+    const T H = (Delta * pr * pr - P * PiD + pth * pth + Q * Q) * hiS;  // 0 on the light cone
+    // dx/dlambda = dH/dp
+    const T dr = Delta * pr * iS;
+    const T dth = pth * iS;
+    const T dph = (Q * is - a * PiD) * iS;
+    // dF/dr at fixed momenta and dG/dtheta
+    const T dF = T(2) * (r - M) * (pr * pr + PiD * PiD) - T(4) * r * pt * PiD;
+    const T dG = T(2) * Q * c * (a * pt - pph * is * is);
+    // dp/dlambda = -dH/dx, with dSigma/dr = 2r and dSigma/dtheta = -2 a^2 sin cos
+    const T dpr = H * T(2) * r * iS - dF * hiS;
+    const T dpth = -(dG * hiS + H * T(2) * a2 * s * c * iS);
+    return Vec5<T>{dr, dth, dph, dpr, dpth};
 }
 
 }  // namespace grrt_b200
