@@ -64,6 +64,8 @@ def parse():
     # smaller frames of the same scene, for profiler captures (default: the benchmark frame)
     ap.add_argument("--width", type=int, default=1024)
     ap.add_argument("--height", type=int, default=1024)
+    # the batched sweep (64 cameras, one persistent launch) instead of the headline frame
+    ap.add_argument("--batch", action="store_true")
     return ap.parse_args()
 
 
@@ -192,9 +194,80 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def run_batch(args):
+    """Batched sweep: spins {0 (Schwarzschild), 0.5, 0.9, 0.998} x 16 inclinations
+    5..90 deg, 256x256 each, thin disk ISCO..20 M, stars seed 42, tolerance 1e-8:
+    one persistent launch (CUDA graph, autotuned schedule) against 64 separate
+    single-camera launches of the same cameras."""
+    import torch
+    import grrt_b200 as G
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
+    cams = G.sweep_cameras()
+    rays = sum(c["width"] * c["height"] for c in cams)
+    B = G.Batch(cams)
+    B.set_precision(form)
+    cache = os.path.join(ROOT, "_build", "batch_schedule_cache.jsonl")
+    os.makedirs(os.path.dirname(cache), exist_ok=True)
+    tuned_ms = B.autotune(cache)
+    out = torch.empty((rays, 4), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        B.render_device(out, stream)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            B.render_device(out, stream)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    st = B.stats()
+    # the same 64 cameras as 64 separate launches (one context each)
+    ctxs = [G.Renderer(c) for c in cams]
+    for R in ctxs:
+        R.set_precision(form)
+    bufs = [torch.empty((c["height"], c["width"], 4), dtype=torch.float32, device="cuda") for c in cams]
+    for _ in range(max(1, args.warmup)):
+        for R, b in zip(ctxs, bufs):
+            R.render_device(b, None, None, stream)
+    torch.cuda.synchronize()
+    sep = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for R, b in zip(ctxs, bufs):
+                R.render_device(b, None, None, stream)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        sep.append(e0.elapsed_time(e1))
+    sep_ms = float(np.mean(sep))
+    chunk, order, bps = B.schedule()
+    line = {"metric": "batched sweep rays/s (64 Kerr cameras x 256^2, one persistent launch)", "value": rays / (ms * 1e-3),
+            "unit": "rays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f64" if form == G.FORM_FP64 else "f32+f64", "data": "synthetic",
+            "config": {"workload": "sweep_64cams_spins0_0.5_0.9_0.998_x16incl_5to90deg_256x256_thin_disk_stars",
+                       "rays_per_step": rays, "schedule": {"chunk": chunk, "order": ["camera-major", "round-robin"][order],
+                                                           "blocks_per_sm": bps, "autotune_ms": tuned_ms},
+                       "l2": "flushed between steps"},
+            "separate_launches_ms_per_step": sep_ms, "batched_speedup": sep_ms / ms,
+            "work": {"attempts_per_ray": st["attempts"] / max(1, st["rays"])}, "gpu_launches": args.steps}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global W, H, RAYS, WORKLOAD
     args = parse()
+    if args.batch:
+        run_batch(args)
+        return
     if (args.width, args.height) != (W, H):
         W, H = args.width, args.height
         RAYS = W * H * SPP

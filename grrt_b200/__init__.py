@@ -120,6 +120,16 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
+        "grrt_batch_create": (vp, [P(GRRTParams), C.c_int]),
+        "grrt_batch_destroy": (None, [vp]),
+        "grrt_batch_error": (C.c_char_p, [vp]),
+        "grrt_batch_set_precision": (C.c_int, [vp, C.c_int]),
+        "grrt_batch_set_schedule": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+        "grrt_batch_get_schedule": (C.c_int, [vp, P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "grrt_batch_autotune": (C.c_int, [vp, C.c_char_p, P(C.c_double)]),
+        "grrt_batch_render": (C.c_int, [vp, P(P(C.c_float))]),
+        "grrt_batch_render_device": (C.c_int, [vp, vp, vp]),
+        "grrt_batch_get_stats": (C.c_int, [vp, P(GRRTStats)]),
         "grrt_scene_table": (C.c_longlong, [vp, C.c_char_p, P(C.c_double), C.c_longlong]),
         "grrt_camera_ray": (C.c_int, [vp, C.c_double, C.c_double, P(C.c_double)]),
     }
@@ -313,6 +323,93 @@ class Renderer:
         out = np.empty(8, dtype=np.float64)
         self._L.grrt_camera_ray(self.ctx, x, y, _dptr(out))
         return out
+
+
+class Batch:
+    """Many thin-disk cameras rendered by one persistent launch (grrt_batch_*)."""
+
+    ORDER_CAMERA_MAJOR = 0
+    ORDER_ROUND_ROBIN = 1
+
+    def __init__(self, cameras: Sequence[dict]):
+        self._L = lib()
+        self.cameras = [dict(c) for c in cameras]
+        arr = (GRRTParams * len(cameras))()
+        for i, c in enumerate(cameras):
+            arr[i] = make_params(c)
+        self.b = self._L.grrt_batch_create(arr, len(cameras))
+        if not self.b:
+            err = self._L.grrt_batch_error(None)
+            raise RuntimeError("grrt_batch_create failed: " + (err.decode() if err else "unknown"))
+        self.sizes = [(c["width"], c["height"]) for c in cameras]
+        self.offsets = np.cumsum([0] + [w * h for w, h in self.sizes])
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            self._L.grrt_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            err = self._L.grrt_batch_error(self.b)
+            raise RuntimeError(f"{what} failed: " + (err.decode() if err else f"rc={rc}"))
+
+    def set_precision(self, form: int) -> None:
+        self._check(self._L.grrt_batch_set_precision(self.b, form), "grrt_batch_set_precision")
+
+    def set_schedule(self, chunk: int, order: int, blocks_per_sm: int = 0) -> None:
+        self._check(self._L.grrt_batch_set_schedule(self.b, chunk, order, blocks_per_sm), "grrt_batch_set_schedule")
+
+    def schedule(self) -> tuple:
+        a, b_, c = C.c_int(), C.c_int(), C.c_int()
+        self._L.grrt_batch_get_schedule(self.b, C.byref(a), C.byref(b_), C.byref(c))
+        return a.value, b_.value, c.value
+
+    def autotune(self, cache_path: Optional[str] = None) -> float:
+        ms = C.c_double()
+        self._check(self._L.grrt_batch_autotune(self.b, cache_path.encode() if cache_path else None, C.byref(ms)),
+                    "grrt_batch_autotune")
+        return ms.value
+
+    def render(self) -> list:
+        fbs = [np.empty((h, w, 4), dtype=np.float32) for w, h in self.sizes]
+        ptrs = (C.POINTER(C.c_float) * len(fbs))(*[f.ctypes.data_as(C.POINTER(C.c_float)) for f in fbs])
+        self._check(self._L.grrt_batch_render(self.b, ptrs), "grrt_batch_render")
+        return fbs
+
+    def render_device(self, d_rgba, stream=None) -> None:
+        p = d_rgba if isinstance(d_rgba, int) else d_rgba.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_batch_render_device(self.b, p, s), "grrt_batch_render_device")
+
+    def stats(self) -> dict:
+        st = GRRTStats()
+        self._check(self._L.grrt_batch_get_stats(self.b, C.byref(st)), "grrt_batch_get_stats")
+        return st.as_dict()
+
+
+def sweep_cameras(width: int = 256, height: int = 256, spins=(0.0, 0.5, 0.9, 0.998), n_incl: int = 16,
+                  incl_lo_deg: float = 5.0, incl_hi_deg: float = 90.0) -> list:
+    """The batched benchmark sweep: spins x evenly spaced inclinations, thin disk
+    ISCO..20 M, stars seed 42, tolerance 1e-8. Spin 0 uses the Schwarzschild
+    metric (with GRRT_METRIC_KERR a spin of 0 selects 0.998)."""
+    cams = []
+    for spin in spins:
+        for k in range(n_incl):
+            th = incl_lo_deg + k * (incl_hi_deg - incl_lo_deg) / (n_incl - 1)
+            p = config_params(2, width=width, height=height, spp=1, observer_theta=math.radians(th))
+            if spin == 0.0:
+                p.update(metric_type=METRIC_SCHWARZSCHILD, spin=0.0)
+            else:
+                p.update(spin=spin)
+            cams.append(p)
+    return cams
 
 
 def cuda_available() -> bool:

@@ -44,6 +44,11 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
                                    const SpectralOutputs& out, const LaunchResources& res, int form,
                                    cudaStream_t stream);
 
+// Batched thin-disk render over many cameras (see DevBatch).
+cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,
+                              int blocks, cudaStream_t stream);
+int thin_batch_max_blocks_per_sm(int form);
+
 // Spectral render whose scratch is a file-scope device array (no allocation);
 // see vol_render.cu. Returns cudaErrorInvalidValue when nb exceeds the limit.
 cudaError_t launch_volume_spectral_noalloc(const DevScene& S, const DevTile& tile, const double* freqs, int nb,

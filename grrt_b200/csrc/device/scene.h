@@ -93,6 +93,28 @@ struct DevTile {
     int out_pitch = 0;
 };
 
+// Batched form: one launch over many cameras. Items are camera images (or
+// tiles of them); the work is cut into chunks of consecutive pixels of one
+// item, and the chunk table fixes the order lanes take them in.
+struct DevBatchItem {
+    int scene = 0;               // index into DevBatch::scenes
+    int x0 = 0, y0 = 0, w = 0, h = 0;
+    int out_pitch = 0;           // output row pitch in pixels
+    size_t out_offset = 0;       // first output pixel of this item
+};
+struct DevBatchChunk {
+    int item = 0;
+    int start = 0;               // first pixel (row-major within the item)
+    int count = 0;               // pixels in this chunk (<= chunk_size)
+};
+struct DevBatch {
+    const DevScene* scenes = nullptr;
+    const DevBatchItem* items = nullptr;
+    const DevBatchChunk* chunks = nullptr;
+    int n_chunks = 0;
+    int chunk_size = 1;
+};
+
 // Per-launch counters (summed over all threads with one atomic per warp).
 struct DevStats {
     unsigned long long attempts;      // DP45 attempts

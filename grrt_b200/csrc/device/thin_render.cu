@@ -68,20 +68,29 @@ __device__ __forceinline__ int start_check(const DevScene& S, int step, double r
 
 }  // namespace
 
-template <int kForm>
-__global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
-thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
-                   double* __restrict__ out_rgb64, uint32_t* __restrict__ out_fate,
-                   unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
-                   const volatile int* __restrict__ cancel) {
+// The per-lane pixel loop shared by the single-camera and the batched kernels.
+// kBatch = false: every lane renders pixels of one camera (scene S0, the
+// kernel's parameter) in the rectangle `tile`, work index = pixel index.
+// kBatch = true: work index -> (chunk, offset) through the batch's chunk table,
+// so one launch covers many cameras (scenes[item.scene]) in the order the
+// schedule lists the chunks.
+template <int kForm, bool kBatch>
+__device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B, const DevTile& tile,
+                                          float4* __restrict__ out_rgba, double* __restrict__ out_rgb64,
+                                          uint32_t* __restrict__ out_fate, unsigned total,
+                                          unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
+                                          const volatile int* __restrict__ cancel) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
-    const int grid2 = S.grid * S.grid;
+    // the scene of the lane's current pixel (batch: per lane, in global memory)
+    int scene = 0;
+#define S (kBatch ? B.scenes[scene] : S0)
+    int px_i = 0, px_j = 0;   // image coordinates of the lane's pixel
+    size_t px_out = 0;        // output index of the lane's pixel
 
     LaneCounters cnt;
     // pixel slot
-    int pix = -1;        // pixel index within the tile; -1 = needs a pixel; -2 = queue exhausted
+    int pix = -1;        // work index of the lane's pixel; -1 = needs a pixel; -2 = queue exhausted
     int smp = 0;         // sample index within the pixel
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     // ray slot
@@ -106,9 +115,30 @@ thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float
             if (want) {
                 const unsigned q = base + __popc(want_mask & lt_mask);
                 if (q < total) {
-                    pix = static_cast<int>(q);
-                    smp = 0;
-                    acc0 = acc1 = acc2 = 0.0;
+                    if (kBatch) {
+                        const DevBatchChunk ch = B.chunks[q / B.chunk_size];
+                        const int within = static_cast<int>(q % B.chunk_size);
+                        if (within < ch.count) {
+                            const DevBatchItem it = B.items[ch.item];
+                            const int local = ch.start + within;
+                            const int qx = local % it.w, qy = local / it.w;
+                            scene = it.scene;
+                            px_i = it.x0 + qx;
+                            px_j = it.y0 + qy;
+                            px_out = it.out_offset + static_cast<size_t>(qy) * it.out_pitch + qx;
+                            pix = static_cast<int>(q);
+                            smp = 0;
+                            acc0 = acc1 = acc2 = 0.0;
+                        }  // else: padding slot of a short chunk, fetch again
+                    } else {
+                        const int qx = static_cast<int>(q) % tile.w, qy = static_cast<int>(q) / tile.w;
+                        px_i = tile.x0 + qx;
+                        px_j = tile.y0 + qy;
+                        px_out = static_cast<size_t>(qy) * tile.out_pitch + qx;
+                        pix = static_cast<int>(q);
+                        smp = 0;
+                        acc0 = acc1 = acc2 = 0.0;
+                    }
                 } else {
                     pix = -2;
                 }
@@ -116,8 +146,7 @@ thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float
         }
         // ---- start a ray for lanes that have a pixel but no live ray ----
         if (!live && pix >= 0) {
-            const int qx = pix % tile.w, qy = pix / tile.w;
-            const int i = tile.x0 + qx, j = tile.y0 + qy;
+            const int i = px_i, j = px_j;
             const int sy = smp / S.grid, sx = smp % S.grid;
             const double x = i + (sx + pixel_hash(i, j, smp, 0)) * S.cell;
             const double yy = j + (sy + pixel_hash(i, j, smp, 1)) * S.cell;
@@ -206,13 +235,13 @@ thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float
             acc0 = acc0 + col0;
             acc1 = acc1 + col1;
             acc2 = acc2 + col2;
+            const int grid2 = S.grid * S.grid;
             if (out_fate) {
                 const unsigned nc = (ncross > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(ncross);
                 out_fate[static_cast<size_t>(pix) * grid2 + smp] = static_cast<unsigned>(term) | (nc << 2);
             }
             if (++smp == grid2) {
-                const int qx = pix % tile.w, qy = pix / tile.w;
-                const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
+                const size_t o = px_out;
                 const double r0 = acc0 * S.inv_spp, r1 = acc1 * S.inv_spp, r2 = acc2 * S.inv_spp;
                 if (out_rgba) out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1),
                                                          static_cast<float>(r2), 1.0f);
@@ -238,7 +267,28 @@ thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float
         // ---- exit when the queue is drained and no lane holds a ray ----
         if (!__any_sync(kFull, live || pix >= -1)) break;
     }
+#undef S
     flush_counters(stats, cnt, cancelled);
+}
+
+template <int kForm>
+__global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
+thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
+                   double* __restrict__ out_rgb64, uint32_t* __restrict__ out_fate,
+                   unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
+                   const volatile int* __restrict__ cancel) {
+    const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
+    thin_loop<kForm, false>(S, DevBatch{}, tile, out_rgba, out_rgb64, out_fate, total, queue, stats, cancel);
+}
+
+// One launch over many cameras: the batched form. Work index space =
+// n_chunks * chunk_size (short chunks padded).
+template <int kForm>
+__global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
+thin_batch_kernel(const __grid_constant__ DevBatch B, float4* __restrict__ out_rgba, unsigned int* __restrict__ queue,
+                  DevStats* __restrict__ stats) {
+    const unsigned total = static_cast<unsigned>(B.n_chunks) * static_cast<unsigned>(B.chunk_size);
+    thin_loop<kForm, true>(B.scenes[0], B, DevTile{}, out_rgba, nullptr, nullptr, total, queue, stats, nullptr);
 }
 
 template <int kForm>
@@ -269,6 +319,27 @@ cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutput
                         const LaunchResources& res, int form, cudaStream_t stream) {
     if (form == kFormMixed) return launch_thin_form<kFormMixed>(S, tile, out, res, stream);
     return launch_thin_form<kFormFP64>(S, tile, out, res, stream);
+}
+
+int thin_batch_max_blocks_per_sm(int form) {
+    int n = 0;
+    if (form == kFormMixed)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel<kFormMixed>, kThreads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel<kFormFP64>, kThreads, 0);
+    return n < 1 ? 1 : n;
+}
+
+cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,
+                              int blocks, cudaStream_t stream) {
+    if (B.n_chunks <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+    if (form == kFormMixed)
+        thin_batch_kernel<kFormMixed><<<blocks, kThreads, 0, stream>>>(B, out_rgba, queue, stats);
+    else
+        thin_batch_kernel<kFormFP64><<<blocks, kThreads, 0, stream>>>(B, out_rgba, queue, stats);
+    return cudaGetLastError();
 }
 
 }  // namespace grrt_b200

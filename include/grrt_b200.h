@@ -89,6 +89,40 @@ GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double* d_spec, in
 GRRT_EXPORT int grrt_render_spectral_device_noalloc(GRRTContext* ctx, const double* d_freqs, int num_bins,
                                                     double* d_spec, int width, int height, void* stream);
 
+/* ---- Batched form: many thin-disk cameras in one persistent launch ----
+ * No counterpart in the reference (it renders one camera per grrt_create).
+ * Each camera is described by its own GRRTParams and keeps the reference's
+ * per-camera semantics exactly (tables, jitter, spp). All pixels of all
+ * cameras go through one device work queue, so long rays of one camera
+ * overlap with short rays of the others; the launch is replayed as a CUDA
+ * graph. Volumetric cameras are rejected. */
+typedef struct GRRTBatch GRRTBatch;
+
+/* Chunk orders of the schedule: all chunks of camera 0, then camera 1, ...;
+ * or chunk k of every camera before chunk k+1. */
+#define GRRT_BATCH_ORDER_CAMERA_MAJOR 0
+#define GRRT_BATCH_ORDER_ROUND_ROBIN 1
+
+/* params: count cameras. NULL on failure with the reason in grrt_batch_error(NULL). */
+GRRT_EXPORT GRRTBatch* grrt_batch_create(const GRRTParams* params, int count);
+GRRT_EXPORT void grrt_batch_destroy(GRRTBatch* batch);
+GRRT_EXPORT const char* grrt_batch_error(const GRRTBatch* batch);
+GRRT_EXPORT int grrt_batch_set_precision(GRRTBatch* batch, int form);
+/* Work is cut into chunks of chunk_size consecutive pixels of one camera;
+ * blocks_per_sm 0 = as many as fit. */
+GRRT_EXPORT int grrt_batch_set_schedule(GRRTBatch* batch, int chunk_size, int order, int blocks_per_sm);
+GRRT_EXPORT int grrt_batch_get_schedule(const GRRTBatch* batch, int* chunk_size, int* order, int* blocks_per_sm);
+/* Times candidate schedules (chunk 64..4096, both orders, two occupancies) and
+ * keeps the fastest; cache_path (may be NULL) stores and reuses the choice for
+ * an identical batch. best_ms may be NULL. */
+GRRT_EXPORT int grrt_batch_autotune(GRRTBatch* batch, const char* cache_path, double* best_ms);
+/* framebuffers[i]: float[W_i*H_i*4] host buffer of camera i (NULL skips it). */
+GRRT_EXPORT int grrt_batch_render(GRRTBatch* batch, float* const* framebuffers);
+/* d_rgba: device float4 buffer of sum(W_i*H_i) pixels, camera i at the prefix
+ * offset sum_{k<i} W_k*H_k. Enqueued on stream. */
+GRRT_EXPORT int grrt_batch_render_device(GRRTBatch* batch, float* d_rgba, void* stream);
+GRRT_EXPORT int grrt_batch_get_stats(GRRTBatch* batch, GRRTStats* out);
+
 /* Counters of the last render; synchronises the context's device. */
 GRRT_EXPORT int grrt_get_stats(GRRTContext* ctx, GRRTStats* out);
 
