@@ -48,6 +48,7 @@ GRRTContext::~GRRTContext() {
         cudaFree(d_out);
         cudaFree(d_freqs);
         cudaFree(d_spec_scratch);
+        cudaFree(d_mixed_scratch);
         if (h_cancel) cudaFreeHost(h_cancel);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -316,8 +317,27 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     out.rgb64 = d_rgb64;
     out.fate = d_fate;
     const DevScene S = scene_for_launch();
+    const bool mixed_thin = !vol && form == GRRT_FORM_MIXED;
+    size_t mixed_bytes = 0;
+    if (mixed_thin) {
+        mixed_bytes = mixed_scratch_bytes(tile, S.grid * S.grid);
+        if (mixed_bytes > d_mixed_scratch_bytes) {
+            cudaFree(d_mixed_scratch);
+            d_mixed_scratch = nullptr;
+            d_mixed_scratch_bytes = 0;
+            if (fail_cuda(cudaMalloc(&d_mixed_scratch, mixed_bytes), "cudaMalloc(mixed scratch)")) return -1;
+            d_mixed_scratch_bytes = mixed_bytes;
+        }
+    }
     cudaEventRecord(ev0, s);
-    cudaError_t e = vol ? launch_volume_rgb(S, tile, out, res, form, s) : launch_thin(S, tile, out, res, form, s);
+    cudaError_t e;
+    if (vol)
+        e = launch_volume_rgb(S, tile, out, res, form, s);
+    else if (mixed_thin)
+        e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
+                              mixed_r_factor * r_horizon, s);
+    else
+        e = launch_thin(S, tile, out, res, form, s);
     cudaEventRecord(ev1, s);
     if (fail_cuda(e, "render launch")) return -1;
     return 0;

@@ -36,6 +36,7 @@ struct GRRTContext {
     int form = GRRT_FORM_FP64;
     double mixed_r_factor = 3.0;
     double tol_fp32 = 1e-6;
+    double mixed_margin = 0.05;  // disk-radius margin (M) of the mixed form's re-trace test
 
     std::string error;
     float progress = 0.0f;
@@ -59,6 +60,8 @@ struct GRRTContext {
     size_t d_freqs_n = 0;
     double* d_spec_scratch = nullptr;
     size_t d_spec_scratch_n = 0;
+    void* d_mixed_scratch = nullptr;
+    size_t d_mixed_scratch_bytes = 0;
 
     GRRTContext() = default;
     ~GRRTContext();

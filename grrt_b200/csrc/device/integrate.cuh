@@ -91,9 +91,8 @@ GRRT_HD T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5
 // so round-off does not accumulate along the ray. The error norm is formed in
 // FP32; its noise floor (about 1e-7 of |h k|/|y|) is why FP32 steps are
 // controlled against their own tolerance (DevScene::tol_fp32).
-__device__ __forceinline__ double mixed_attempt_impl(float M, float a, float pt, float pph,
-                                                     const Vec5<double>& y, double dl,
-                                                     Vec5<double>& y5) {
+GRRT_HD double mixed_attempt_impl(float M, float a, float pt, float pph, const Vec5<double>& y, double dl,
+                                  Vec5<double>& y5, Vec5<float>& k7_out) {
     using namespace dp;
     const Vec5<float> yf{static_cast<float>(y.r), static_cast<float>(y.th), static_cast<float>(y.ph),
                          static_cast<float>(y.pr), static_cast<float>(y.pth)};
@@ -128,6 +127,7 @@ __device__ __forceinline__ double mixed_attempt_impl(float M, float a, float pt,
     const Vec5<float> y5f{static_cast<float>(y5.r), static_cast<float>(y5.th), static_cast<float>(y5.ph),
                           static_cast<float>(y5.pr), static_cast<float>(y5.pth)};
     const Vec5<float> k7 = kerr_rhs<float>(M, a, pt, pph, y5f);
+    k7_out = k7;
     float err = 0.0f;
 #define GRRT_ERRF(f)                                                                     \
     {                                                                                    \
@@ -149,14 +149,18 @@ struct StepDecision {
 // step, on which the solution depends through the truncation error (a relative
 // change d in the step moves the result by about 5 d times the local error), so
 // single precision (2^-22 relative) is ample and avoids an FP64 pow per attempt.
-__device__ __forceinline__ double step_factor_pow(double x) {
+GRRT_HD double step_factor_pow(double x) {
+#ifdef __CUDA_ARCH__
     return static_cast<double>(__powf(static_cast<float>(x), 0.2f));
+#else
+    return static_cast<double>(powf(static_cast<float>(x), 0.2f));
+#endif
 }
 
 // retry = number of rejected attempts so far in this outer step (0..20). The
 // 21st attempt (retry == 20) is taken unconditionally with next = dl, as the
 // reference's "exhausted retries" path.
-__device__ __forceinline__ StepDecision pi_control(double err, double tol, double dl, int retry,
+GRRT_HD StepDecision pi_control(double err, double tol, double dl, int retry,
                                                    double r5) {
     constexpr double safety = 0.9, grow_max = 5.0, shrink_max = 0.2, dl_min = 1e-6;
     StepDecision d;

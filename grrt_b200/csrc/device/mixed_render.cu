@@ -1,0 +1,448 @@
+// Mixed-precision form of the thin-disk render: speculate in FP32, re-trace in
+// FP64 the samples whose colour depends on the FP64 step sequence (the tests
+// are in mixed_spec.cuh).
+//
+//   speculate: every sample is integrated with FP32 right-hand sides and FP64
+//     state (mixed_attempt_impl) against a relaxed tolerance. A sample that
+//     needs the FP64 step sequence is queued for the re-trace and dropped; a
+//     horizon sample is final (colour 0); an escape stores its sky arc for the
+//     star pass.
+//   stars: each pending escape checks the star catalogue along its arc; a
+//     star in reach queues it for the re-trace, otherwise its colour is 0.
+//     (Its own pass, so the speculative warps never diverge into the star scan.)
+//   re-trace: the queued samples are traced from the camera with the plain
+//     form's arithmetic, lanes pulling from the queue (converged FP64 warps).
+//   resolve: per pixel, the spp samples are summed in order and scaled, as
+//     Renderer::render does (src/renderer.cpp:47-72).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "integrate.cuh"
+#include "mixed_spec.cuh"
+#include "render_launch.h"
+#include "shading.cuh"
+
+namespace grrt_b200 {
+
+namespace {
+
+constexpr int kMixThreads = 128;
+constexpr unsigned kMask = 0xffffffffu;
+
+__device__ __forceinline__ void sample_start(const DevScene& S, const DevTile& tile, unsigned q, int g2,
+                                             Vec5<double>& y, double& pt, double& pph) {
+    const int pix = static_cast<int>(q / g2), s = static_cast<int>(q % g2);
+    const int i = tile.x0 + pix % tile.w, j = tile.y0 + pix / tile.w;
+    const int sy = s / S.grid, sx = s % S.grid;
+    const double x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
+    const double yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;
+    double p[4];
+    camera_momentum(S, x, yy, p);
+    y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], p[1], p[2]};
+    pt = p[0];
+    pph = p[3];
+}
+
+// True when the star lookup at any point of the arc could find a star: one
+// scan of the cells every lookup along it can reach (the arc's cell span plus
+// the lookup's one-cell border), with a point-to-segment distance per star
+// against the lookup tolerance plus 1e-4 rad of slack (far-field model and
+// FP32 trajectory). Arcs near a pole, where the picture and the cell scan
+// break down, count as in reach.
+__device__ bool star_in_reach(const DevStars& st, const mixed::EscapeArc& e) {
+    double th0 = e.th0, ph0 = e.ph0;
+    double th1 = e.th0 + e.dth, ph1 = e.ph0 + e.dph;
+    const bool f0 = mixed::fold_sky(th0, ph0), f1 = mixed::fold_sky(th1, ph1);
+    constexpr double kCell = kPiD / 180.0;  // star grid cells are 1 degree
+    if (f0 != f1 || fmin(th0, th1) < 3.0 * kCell || fmax(th0, th1) > kPiD - 3.0 * kCell) return true;
+    double dph = ph1 - ph0;
+    if (dph > kPiD) dph -= 2.0 * kPiD;
+    if (dph < -kPiD) dph += 2.0 * kPiD;
+    if (fabs(dph) > 10.0 * kCell || fabs(th1 - th0) > 10.0 * kCell) return true;
+    // the lookup's distance metric weighs phi by sin(theta): take its smallest
+    // value along the segment (sin is concave on [0, pi])
+    const double s = fmin(sin(th0), sin(th1));
+    const double tol = sqrt(st.tol2) + 1e-4;
+    const double ex = th1 - th0, ey = dph * s;
+    const double e2 = ex * ex + ey * ey;
+    constexpr int nt = 180, np = 360;
+    const int t_lo = max(static_cast<int>(fmin(th0, th1) * nt / kPiD) - 1, 0);
+    const int t_hi = min(static_cast<int>(fmax(th0, th1) * nt / kPiD) + 1, nt - 1);
+    const double pa = fmin(ph0, ph0 + dph), pb = fmax(ph0, ph0 + dph);
+    const int p_lo = static_cast<int>(floor((pa + kPiD) * np / (2.0 * kPiD))) - 1;
+    const int p_hi = static_cast<int>(floor((pb + kPiD) * np / (2.0 * kPiD))) + 1;
+    for (int t = t_lo; t <= t_hi; ++t) {
+        for (int pc = p_lo; pc <= p_hi; ++pc) {
+            const int cell = t * np + ((pc % np) + np) % np;
+            const int q1 = __ldg(st.cell_start + cell + 1);
+            for (int q = __ldg(st.cell_start + cell); q < q1; ++q) {
+                const int si = __ldg(st.cell_items + q);
+                const double qx = __ldg(st.theta + si) - th0;
+                double qp = __ldg(st.phi + si) - ph0;
+                if (qp > kPiD) qp -= 2.0 * kPiD;
+                if (qp < -kPiD) qp += 2.0 * kPiD;
+                const double qy = qp * s;
+                double t_seg = e2 > 0.0 ? (qx * ex + qy * ey) / e2 : 0.0;
+                t_seg = fmin(fmax(t_seg, 0.0), 1.0);
+                const double dx = qx - t_seg * ex, dy = qy - t_seg * ey;
+                if (dx * dx + dy * dy < tol * tol) return true;
+            }
+        }
+    }
+    return false;
+}
+
+// Queues sample q for the FP64 re-trace (warp-aggregated over the lanes that ask).
+__device__ __forceinline__ void queue_retrace(bool want, unsigned q, const DevMixedBuffers& mb) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(kMask, want);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(mb.retrace_count, static_cast<unsigned>(__popc(m)));
+    base = __shfl_sync(kMask, base, leader);
+    if (want) mb.retrace_list[base + __popc(m & ((1u << lane) - 1u))] = q;
+}
+
+__device__ __forceinline__ int start_test(const DevScene& S, int step, double r) {
+    if (step >= S.max_steps) return kTermMaxSteps;
+    if (r < S.r_stop) return kTermHorizon;
+    if (r > S.r_escape) return kTermEscaped;
+    return -1;
+}
+
+__device__ __forceinline__ void warp_add(DevStats* st, unsigned long long a, unsigned long long acc,
+                                         unsigned long long rays, unsigned long long f64) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(kMask, a, o);
+        acc += __shfl_xor_sync(kMask, acc, o);
+        rays += __shfl_xor_sync(kMask, rays, o);
+        f64 += __shfl_xor_sync(kMask, f64, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&st->attempts, a);
+        atomicAdd(&st->accepted, acc);
+        atomicAdd(&st->rays, rays);
+        atomicAdd(&st->fp64_attempts, f64);
+    }
+}
+
+// Warp-aggregated fetch of the next work index; returns ~0u when exhausted.
+__device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned total) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(kMask, want);
+    unsigned base = 0;
+    if (m) {
+        const int leader = __ffs(m) - 1;
+        if (lane == leader) base = atomicAdd(counter, static_cast<unsigned>(__popc(m)));
+        base = __shfl_sync(kMask, base, leader);
+    }
+    if (!want) return ~0u;
+    const unsigned q = base + __popc(m & ((1u << lane) - 1u));
+    return q < total ? q : ~0u;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kMixThreads, 4)
+mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb, DevStats* stats) {
+    const int g2 = S.grid * S.grid;
+    const unsigned total = static_cast<unsigned>(tile.w) * tile.h * g2;
+    const float Mf = static_cast<float>(S.M), af = static_cast<float>(S.a);
+    unsigned long long n_att = 0, n_acc = 0, n_rays = 0;
+    unsigned q = ~0u;
+    bool live = false, exhausted = false;
+    Vec5<double> y;
+    double pt = 0, pph = 0, dl = 0;
+    int retry = 0, step = 0;
+    mixed::Tracker trk;
+    while (true) {
+        const bool want = !live && !exhausted;
+        const unsigned nq = fetch(want, mb.queue, total);
+        if (want) {
+            if (nq == ~0u) {
+                exhausted = true;
+            } else {
+                q = nq;
+                sample_start(S, tile, q, g2, y, pt, pph);
+                dl = S.dl0;
+                retry = 0;
+                step = 0;
+                trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near);
+                live = true;
+            }
+        }
+        if (!__any_sync(kMask, live)) break;
+        int term = -1;
+        bool retrace = false;
+        Vec5<float> k7;
+        if (live && retry == 0) term = start_test(S, step, y.r);
+        if (live && term < 0) {
+            Vec5<double> y5;
+            const double err =
+                mixed_attempt_impl(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, y5, k7);
+            ++n_att;
+            const StepDecision d = pi_control(err, S.tol_fp32, dl, retry, y5.r);
+            if (d.accept) {
+                ++n_acc;
+                retrace = trk.step(y, y5);
+                y = y5;
+                dl = d.next;
+                retry = 0;
+                ++step;
+                term = retrace ? kTermMaxSteps : start_test(S, step, y.r);
+            } else {
+                dl = d.next;
+                ++retry;
+            }
+        }
+        bool queue = false;
+        if (live && term >= 0) {
+            live = false;
+            ++n_rays;
+            const size_t o = 3 * static_cast<size_t>(q);
+            if (retrace || term == kTermMaxSteps) {
+                queue = true;
+            } else if (term == kTermEscaped && S.stars_on) {
+                // an escape always ends an accepted step, so k7 is the
+                // right-hand side at y
+                const mixed::EscapeArc e = mixed::escape_arc(S.r_escape, y, k7);
+                mb.sample_rgb[o + 0] = e.th0;
+                mb.sample_rgb[o + 1] = e.ph0;
+                mb.sample_rgb[o + 2] = __hiloint2double(__float_as_int(e.dth), __float_as_int(e.dph));
+                mb.sample_fate[q] = mixed::kFateStarPending;
+            } else {
+                // horizon, or an escape with stars off: colour 0
+                mb.sample_rgb[o + 0] = 0.0;
+                mb.sample_rgb[o + 1] = 0.0;
+                mb.sample_rgb[o + 2] = 0.0;
+                mb.sample_fate[q] = static_cast<unsigned>(term);
+            }
+        }
+        queue_retrace(queue, q, mb);
+    }
+    warp_add(stats, n_att, n_acc, n_rays, 0ull);
+}
+
+// Star pass over the pending escapes: colour 0, or queued for the re-trace.
+__global__ void __launch_bounds__(256)
+mixed_star_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb) {
+    const unsigned n = static_cast<unsigned>(tile.w) * tile.h * (S.grid * S.grid);
+    const unsigned stride = gridDim.x * blockDim.x;
+    // whole warps iterate together so queue_retrace can ballot
+    for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const unsigned q = base + threadIdx.x;
+        bool queue = false;
+        if (q < n && mb.sample_fate[q] == mixed::kFateStarPending) {
+            const size_t o = 3 * static_cast<size_t>(q);
+            mixed::EscapeArc e;
+            e.th0 = mb.sample_rgb[o + 0];
+            e.ph0 = mb.sample_rgb[o + 1];
+            const double packed = mb.sample_rgb[o + 2];
+            e.dth = __int_as_float(__double2hiint(packed));
+            e.dph = __int_as_float(__double2loint(packed));
+            if (star_in_reach(S.stars, e)) {
+                queue = true;
+            } else {
+                mb.sample_rgb[o + 0] = 0.0;
+                mb.sample_rgb[o + 1] = 0.0;
+                mb.sample_rgb[o + 2] = 0.0;
+                mb.sample_fate[q] = static_cast<unsigned>(kTermEscaped);
+            }
+        }
+        queue_retrace(queue, q, mb);
+    }
+}
+
+// FP64 re-trace of the queued samples with the plain form's arithmetic.
+__global__ void __launch_bounds__(kMixThreads, 4)
+mixed_retrace_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb, DevStats* stats) {
+    const int g2 = S.grid * S.grid;
+    const unsigned total = *mb.retrace_count;
+    unsigned long long n_att = 0, n_acc = 0;
+    unsigned q = ~0u;
+    bool live = false, exhausted = false;
+    Vec5<double> y;
+    double pt = 0, pph = 0, dl = 0;
+    int retry = 0, step = 0, ncross = 0;
+    double c0 = 0, c1 = 0, c2 = 0;
+    while (true) {
+        const bool want = !live && !exhausted;
+        const unsigned nq = fetch(want, mb.queue2, total);
+        if (want) {
+            if (nq == ~0u) {
+                exhausted = true;
+            } else {
+                q = mb.retrace_list[nq];
+                sample_start(S, tile, q, g2, y, pt, pph);
+                dl = S.dl0;
+                retry = 0;
+                step = 0;
+                ncross = 0;
+                c0 = c1 = c2 = 0.0;
+                live = true;
+            }
+        }
+        if (!__any_sync(kMask, live)) break;
+        int term = -1;
+        if (live && retry == 0) term = start_test(S, step, y.r);
+        if (live && term < 0) {
+            Vec5<double> y5;
+            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            ++n_att;
+            const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
+            if (d.accept) {
+                ++n_acc;
+                if (S.disk_on) {
+                    const double d_prev = y.th - kHalfPi;
+                    const double d_new = y5.th - kHalfPi;
+                    if (d_prev * d_new < 0.0 && fabs(d_prev - d_new) > 1e-12) {
+                        const double frac = -d_prev / (d_new - d_prev);
+                        const double rc = y.r + frac * (y5.r - y.r);
+                        if (rc >= S.r_in && rc <= S.r_out) {
+                            double e0, e1, e2;
+                            disk_emission(S, rc, pt, pph, e0, e1, e2);
+                            c0 += e0;
+                            c1 += e1;
+                            c2 += e2;
+                            ++ncross;
+                        }
+                    }
+                }
+                y = y5;
+                dl = d.next;
+                retry = 0;
+                ++step;
+                term = start_test(S, step, y.r);
+            } else {
+                dl = d.next;
+                ++retry;
+            }
+        }
+        if (live && term >= 0) {
+            live = false;
+            if (term == kTermEscaped && S.stars_on) {
+                const double b = star_brightness(S.stars, y.th, y.ph);
+                c0 += b;
+                c1 += b;
+                c2 += b;
+            }
+            mb.sample_rgb[3 * static_cast<size_t>(q) + 0] = c0;
+            mb.sample_rgb[3 * static_cast<size_t>(q) + 1] = c1;
+            mb.sample_rgb[3 * static_cast<size_t>(q) + 2] = c2;
+            const unsigned nc = (ncross > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(ncross);
+            mb.sample_fate[q] = static_cast<unsigned>(term) | (nc << 2);
+        }
+    }
+    warp_add(stats, n_att, n_acc, 0ull, n_att);
+}
+
+// Per pixel: sum the spp sample colours in order, scale, write the outputs.
+__global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb,
+                                     float4* __restrict__ out_rgba, double* __restrict__ out_rgb64,
+                                     uint32_t* __restrict__ out_fate, DevStats* stats) {
+    const int g2 = S.grid * S.grid;
+    const unsigned npix = static_cast<unsigned>(tile.w) * tile.h;
+    unsigned long long hz = 0, es = 0, mx = 0, cr = 0;
+    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int s = 0; s < g2; ++s) {
+            const size_t q = static_cast<size_t>(p) * g2 + s;
+            a0 = a0 + mb.sample_rgb[3 * q + 0];
+            a1 = a1 + mb.sample_rgb[3 * q + 1];
+            a2 = a2 + mb.sample_rgb[3 * q + 2];
+            const unsigned f = mb.sample_fate[q];
+            const unsigned t = f & 3u;
+            hz += (t == kTermHorizon);
+            es += (t == kTermEscaped);
+            mx += (t == kTermMaxSteps);
+            cr += f >> 2;
+            if (out_fate) out_fate[q] = f;
+        }
+        const int qx = static_cast<int>(p % tile.w), qy = static_cast<int>(p / tile.w);
+        const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
+        const double r0 = a0 * S.inv_spp, r1 = a1 * S.inv_spp, r2 = a2 * S.inv_spp;
+        if (out_rgba)
+            out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1), static_cast<float>(r2), 1.0f);
+        if (out_rgb64) {
+            out_rgb64[3 * o + 0] = r0;
+            out_rgb64[3 * o + 1] = r1;
+            out_rgb64[3 * o + 2] = r2;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        hz += __shfl_xor_sync(kMask, hz, o);
+        es += __shfl_xor_sync(kMask, es, o);
+        mx += __shfl_xor_sync(kMask, mx, o);
+        cr += __shfl_xor_sync(kMask, cr, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&stats->horizon, hz);
+        atomicAdd(&stats->escaped, es);
+        atomicAdd(&stats->max_steps, mx);
+        atomicAdd(&stats->crossings, cr);
+    }
+}
+
+size_t mixed_scratch_bytes(const DevTile& tile, int g2) {
+    const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
+    return n * (3 * sizeof(double) + 2 * sizeof(unsigned)) + 1024;
+}
+
+cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                              const LaunchResources& res, void* scratch, size_t scratch_bytes, double margin,
+                              double r_near, cudaStream_t stream) {
+    DevStats* stats = res.stats;
+    const int g2 = S.grid * S.grid;
+    const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
+    if (n == 0) return cudaSuccess;
+    if (scratch_bytes < mixed_scratch_bytes(tile, g2)) return cudaErrorInvalidValue;
+    auto* base = static_cast<unsigned char*>(scratch);
+    DevMixedBuffers mb;
+    mb.queue = res.queue;  // the phase-1 counter doubles as the progress counter
+    mb.queue2 = reinterpret_cast<unsigned*>(base + 256);
+    mb.retrace_count = reinterpret_cast<unsigned*>(base + 512);
+    mb.sample_rgb = reinterpret_cast<double*>(base + 1024);
+    mb.sample_fate = reinterpret_cast<uint32_t*>(base + 1024 + n * 3 * sizeof(double));
+    mb.retrace_list = mb.sample_fate + n;
+    mb.margin = margin;
+    mb.r_near = r_near;
+    cudaError_t e = cudaMemsetAsync(base, 0, 1024, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    static int sms = 0, per1 = 0, per2 = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, mixed_speculate_kernel, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, mixed_retrace_kernel, kMixThreads, 0);
+        if (per1 < 1) per1 = 1;
+        if (per2 < 1) per2 = 1;
+    }
+    const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
+    mixed_speculate_kernel<<<need < sms * per1 ? need : sms * per1, kMixThreads, 0, stream>>>(S, tile, mb, stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (S.stars_on) {
+        int sb = static_cast<int>((n + 255) / 256);
+        if (sb > sms * 8) sb = sms * 8;
+        mixed_star_kernel<<<sb, 256, 0, stream>>>(S, tile, mb);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    mixed_retrace_kernel<<<sms * per2, kMixThreads, 0, stream>>>(S, tile, mb, stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t npix = static_cast<size_t>(tile.w) * tile.h;
+    int rb = static_cast<int>((npix + 255) / 256);
+    if (rb > sms * 8) rb = sms * 8;
+    mixed_resolve_kernel<<<rb, 256, 0, stream>>>(S, tile, mb, out.rgba, out.rgb64, out.fate, stats);
+    return cudaGetLastError();
+}
+
+}  // namespace grrt_b200

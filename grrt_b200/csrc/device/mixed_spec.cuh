@@ -1,0 +1,123 @@
+// Decisions of the speculative (FP32) pass of the mixed-precision thin-disk
+// form, shared by the kernels and the host-side tests.
+//
+// A thin-disk sample's colour is exactly 0 (horizon, or escape with no star),
+// exactly a star's brightness, or emission summed at disk crossings whose
+// radius is interpolated between two accepted steps
+// (src/geodesic_tracer.cpp:156-176). Only the last two depend on where the
+// FP64 steps land. The speculative pass integrates every sample with FP32
+// right-hand sides and marks for the FP64 re-trace each sample whose colour
+// the FP64 step sequence could make non-zero or move:
+//   - an equatorial crossing with interpolated radius in [r_in - m, r_out + m]
+//     widened by kCrossStepFrac of the step's radial extent (the interpolated
+//     radius moves with the step placement: chord error);
+//   - an accepted step over those radii closer than kGrazeAbs to the plane, or
+//     a theta turning point there closer than kGrazeTurn (a graze, which the
+//     FP64 steps may turn into a crossing or step over);
+//   - more than kSweptMax radians swept inside r_near (near-critical orbits:
+//     trajectory differences grow about e-fold per radian there);
+//   - the step budget;
+//   - an escape whose star lookup could find a star (see EscapeArc).
+#pragma once
+
+#include "integrate.cuh"
+
+namespace grrt_b200 {
+namespace mixed {
+
+constexpr double kCrossStepFrac = 0.2;
+constexpr double kGrazeAbs = 2e-3;
+constexpr double kGrazeTurn = 0.1;
+constexpr double kSweptMax = 3.0;
+constexpr double kPi = 3.14159265358979323846;
+
+// sample_fate value of an escape whose star test is still to run.
+constexpr unsigned kFateStarPending = 0xffffffffu;
+
+struct Tracker {
+    double lo = 0.0, hi = 0.0, r_near = 0.0;
+    bool disk = false;
+    double swept = 0.0;
+
+    GRRT_HD void reset(bool disk_on, double r_in, double r_out, double margin, double r_near_) {
+        disk = disk_on;
+        lo = r_in - margin;
+        hi = r_out + margin;
+        r_near = r_near_;
+        swept = 0.0;
+    }
+
+    // One accepted step y -> y5; true when the sample needs the FP64 re-trace.
+    GRRT_HD bool step(const Vec5<double>& y, const Vec5<double>& y5) {
+        bool hit = false;
+        if (disk) {
+            const double d_prev = y.th - 0.5 * kPi, d_new = y5.th - 0.5 * kPi;
+            if (d_prev * d_new < 0.0 && fabs(d_prev - d_new) > 1e-12) {
+                const double rc = y.r + (-d_prev / (d_new - d_prev)) * (y5.r - y.r);
+                const double w = kCrossStepFrac * fabs(y5.r - y.r);
+                hit = rc >= lo - w && rc <= hi + w;
+            } else if (y5.r >= lo && y5.r <= hi) {
+                const double m = fmin(fabs(d_prev), fabs(d_new));
+                hit = m < kGrazeAbs || (y.pth * y5.pth <= 0.0 && m < kGrazeTurn);
+            }
+        }
+        if (y.r < r_near) {
+            float s, c;
+            fast_sincos(static_cast<float>(y.th), s, c);
+            swept += fabs(y5.th - y.th) + fabs(y5.ph - y.ph) * static_cast<double>(fabsf(s));
+            if (swept > kSweptMax) hit = true;
+        }
+        return hit;
+    }
+};
+
+// The arc of sky an escaping ray's star lookup can land on. The reference looks
+// the star up at the first accepted step past r_escape, whose radius depends on
+// the step sequence; a step is capped at 5 max(r, 1) in the affine parameter,
+// so it lands below 6 r_escape. In the far field
+// angle(r) = angle_f + c (1/r_f - 1/r) with c = r^2 d(angle)/dr, a straight
+// segment in (theta, phi) from r = r_escape (th0, ph0) to r = 7 r_escape
+// (th0 + dth, ph0 + dph), unfolded (no pole or 2 pi wrap applied).
+struct EscapeArc {
+    double th0, ph0;
+    float dth, dph;
+};
+
+// k = right-hand side at the escape state y (dr, dtheta, dphi used).
+GRRT_HD EscapeArc escape_arc(double r_escape, const Vec5<double>& y, const Vec5<float>& k) {
+    EscapeArc e;
+    const double r_f = y.r;
+    const double dr = static_cast<double>(k.r);
+    const double c_th = dr > 0.0 ? r_f * r_f * static_cast<double>(k.th) / dr : 0.0;
+    const double c_ph = dr > 0.0 ? r_f * r_f * static_cast<double>(k.ph) / dr : 0.0;
+    const double u0 = 1.0 / r_f - 1.0 / r_escape;
+    const double du = (1.0 / r_escape - 1.0 / (7.0 * r_escape));
+    e.th0 = y.th + c_th * u0;
+    e.ph0 = y.ph + c_ph * u0;
+    // a non-outgoing ray (dr <= 0 cannot escape past r_escape in the far field)
+    // gets an arc long enough to be sent to the re-trace
+    e.dth = dr > 0.0 ? static_cast<float>(c_th * du) : 1.0f;
+    e.dph = dr > 0.0 ? static_cast<float>(c_ph * du) : 1.0f;
+    return e;
+}
+
+// Folds (theta, phi) the way the star lookup does (src/celestial_sphere.cpp:48-90):
+// theta into [0, pi] (phi + pi when it passes a pole), phi into [-pi, pi].
+// Returns whether theta was reflected.
+GRRT_HD bool fold_sky(double& theta, double& phi) {
+    theta = fmod(theta, 2.0 * kPi);
+    if (theta < 0.0) theta += 2.0 * kPi;
+    bool flip = false;
+    if (theta > kPi) {
+        theta = 2.0 * kPi - theta;
+        phi += kPi;
+        flip = true;
+    }
+    phi = fmod(phi, 2.0 * kPi);
+    if (phi > kPi) phi -= 2.0 * kPi;
+    if (phi < -kPi) phi += 2.0 * kPi;
+    return flip;
+}
+
+}  // namespace mixed
+}  // namespace grrt_b200

@@ -22,6 +22,18 @@ struct SpectralOutputs {
     uint32_t* fate = nullptr;
 };
 
+// Scratch of the mixed-precision thin-disk form (see mixed_render.cu).
+struct DevMixedBuffers {
+    unsigned* queue = nullptr;          // phase-1 work counter
+    unsigned* queue2 = nullptr;         // phase-2 work counter
+    unsigned* retrace_count = nullptr;  // samples queued for the FP64 re-trace
+    unsigned* retrace_list = nullptr;   // their sample indices
+    double* sample_rgb = nullptr;       // 3 per sample
+    uint32_t* sample_fate = nullptr;    // per sample
+    double margin = 0.05;               // disk-radius margin of the re-trace test
+    double r_near = 0.0;                // escapes after coming inside r_near are re-traced
+};
+
 // Scratch a launch uses beside its inputs and outputs.
 struct LaunchResources {
     unsigned int* queue = nullptr;    // work counter (zeroed by the launcher)
@@ -43,6 +55,12 @@ cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const Thin
 cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
                                    const SpectralOutputs& out, const LaunchResources& res, int form,
                                    cudaStream_t stream);
+
+// Mixed-precision thin-disk render: FP32 speculation, FP64 re-trace, resolve.
+size_t mixed_scratch_bytes(const DevTile& tile, int g2);
+cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                              const LaunchResources& res, void* scratch, size_t scratch_bytes, double margin,
+                              double r_near, cudaStream_t stream);
 
 // Batched thin-disk render over many cameras (see DevBatch).
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,

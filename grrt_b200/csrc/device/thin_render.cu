@@ -172,8 +172,9 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
             double err;
             double tol = S.tol;
             if (kForm == kFormMixed && y.r > S.fp32_r_min) {
+                Vec5<float> k7;
                 err = mixed_attempt_impl(static_cast<float>(S.M), static_cast<float>(S.a),
-                                         static_cast<float>(pt), static_cast<float>(pph), y, dl, y5);
+                                         static_cast<float>(pt), static_cast<float>(pph), y, dl, y5, k7);
                 tol = S.tol_fp32;
             } else {
                 err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);

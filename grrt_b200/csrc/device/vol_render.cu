@@ -185,8 +185,9 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
             Vec5<double> y5;
             double err, tol = S.tol;
             if (kForm == kFormMixed && y.r > S.fp32_r_min) {
+                Vec5<float> k7;
                 err = mixed_attempt_impl(static_cast<float>(S.M), static_cast<float>(S.a), static_cast<float>(pt),
-                                         static_cast<float>(pph), y, dl, y5);
+                                         static_cast<float>(pph), y, dl, y5, k7);
                 tol = S.tol_fp32;
             } else {
                 err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
