@@ -9,12 +9,15 @@ background (5000 stars, seed 42); adaptive Dormand-Prince 5(4) at tolerance
 1024*1024*4 = 4,194,304 rays per step. Inputs are synthetic (the scene is
 generated from its parameters; no dataset).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64]
   python bench.py --impl reference   # the reference's own CPU code, same workload
 
-`value` is rays/s with the scene and the output resident on the device (CUDA
-events around each render launch on its stream; a 256 MiB buffer is written
-between steps to flush the 126 MB L2). `e2e` is the same metric through the
+`value` is rays/s of the headline form (default: mixed, whose output is held
+to <=1e-4 relative of the FP64 form and reported against it) with the scene
+and the output resident on the device (CUDA events around each render launch
+on its stream; a 256 MiB buffer is written between steps to flush the 126 MB
+L2). Both forms are timed; "forms" reports each, with per-kernel phase times
+from the library's own CUDA events. `e2e` is the same metric through the
 reference C entry point grrt_render with a host framebuffer (launch
 parameters in, the float RGBA frame out, every step).
 """
@@ -59,7 +62,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    # headline form; the other form is timed too and reported under "forms"
+    ap.add_argument("--form", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # smaller frames of the same scene, for profiler captures (default: the benchmark frame)
     ap.add_argument("--width", type=int, default=1024)
@@ -262,6 +266,93 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def time_form(torch, R, form, stream, flush, rgba, steps, warmup, dist):
+    """W warm-up frames, then K timed frames of one precision form: CUDA events
+    around each render launch on its stream, plus the library's per-phase events."""
+    R.set_precision(form)
+
+    def step(ev=None):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # evict L2 between frames
+            if ev is not None:
+                ev[0].record(stream)
+            R.render_device(rgba, None, None, stream)
+            if ev is not None:
+                ev[1].record(stream)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    st = R.stats()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    phases = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        step(evs[k])
+        phases.append(R.phase_ms())  # waits for this frame; the next frame is enqueued after
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    kernel_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = float(np.mean(kernel_ms))
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    phase_mean = [float(np.mean([p[k] for p in phases])) for k in range(len(phases[0]))]
+    return {"ms": ms, "kernel_ms": kernel_ms, "stats": st, "phase_ms": phase_mean, "wall": wall}
+
+
+def form_error(torch, grrt, params):
+    """Mixed against FP64 on the benchmark frame: per-pixel relative error of the
+    double colour and the number of samples whose fate differs."""
+    R = grrt.Renderer(params)
+    g2 = SPP
+    out = {}
+    for name, form in (("fp64", grrt.FORM_FP64), ("mixed", grrt.FORM_MIXED)):
+        R.set_precision(form)
+        rgb = torch.empty((H, W, 3), dtype=torch.float64, device="cuda")
+        fate = torch.empty((H * W * g2,), dtype=torch.int32, device="cuda")
+        R.render_device(None, rgb, fate)
+        torch.cuda.synchronize()
+        out[name] = (rgb, fate)
+    f, m = out["fp64"][0], out["mixed"][0]
+    scale = float(f.max())
+    rel = (m - f).abs() / torch.clamp(f.abs(), min=1e-6 * scale)
+    R.close()
+    return {"max_rel": float(rel.max()), "pixels_over_1e-4": int((rel.amax(dim=2) > 1e-4).sum()),
+            "pixels_differing": int(((m != f).any(dim=2)).sum()),
+            "sample_fates_differing": int((out["fp64"][1] != out["mixed"][1]).sum()),
+            "rel_floor": "max(|fp64|, 1e-6 x frame max)"}
+
+
+def sgemm_peak(torch) -> float:
+    """FP32 (non-tensor) roofline denominator: cuBLAS SGEMM 8192^3 with TF32 off, best of 5."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
 def main():
     global W, H, RAYS, WORKLOAD
     args = parse()
@@ -287,52 +378,24 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     import grrt_b200 as G
 
-    form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
-    R = G.Renderer(G.config_params(2, width=W, height=H))
-    R.set_precision(form)
+    params = G.config_params(2, width=W, height=H)
+    R = G.Renderer(params)
     stream = torch.cuda.Stream()
     rgba = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def step(timed_events=None):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)  # evict L2 between frames
-            if timed_events is not None:
-                timed_events[0].record(stream)
-            R.render_device(rgba, None, None, stream)
-            if timed_events is not None:
-                timed_events[1].record(stream)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    st = R.stats()
-    attempts_per_frame = st["attempts"]
-
+    head_form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
+    other_form = G.FORM_FP64 if head_form == G.FORM_MIXED else G.FORM_MIXED
     clocks = ClockSampler(local)
     clocks.start()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        step(evs[k])
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    if dist:
-        dist.barrier()
+    res = {other_form: time_form(torch, R, other_form, stream, flush, rgba, args.steps, args.warmup, dist),
+           head_form: time_form(torch, R, head_form, stream, flush, rgba, args.steps, args.warmup, dist)}
     clk = clocks.stop()
-    kernel_ms = [a.elapsed_time(b) for a, b in evs]
-    ms = float(np.mean(kernel_ms))
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    head = res[head_form]
+    ms = head["ms"]
     value = world * RAYS / (ms * 1e-3)
 
-    # end to end through the reference C entry point (host framebuffer)
+    # end to end through the reference C entry point (host framebuffer), headline form
     host_fb = np.empty((H, W, 4), dtype=np.float32)
     import ctypes as C
     L = G.lib()
@@ -355,20 +418,54 @@ def main():
     e2e = {"value": world * RAYS / e2e_s, "unit": "rays/s",
            "h2d_bytes_per_step": 1536,  # launch parameters (scene description) per frame
            "d2h_bytes_per_step": W * H * 16,  # float RGBA frame
-           "api": "grrt_render(ctx, float* host_framebuffer)", "ms_per_step": 1e3 * e2e_s}
+           "api": "grrt_render(ctx, float* host_framebuffer)", "form": args.form, "ms_per_step": 1e3 * e2e_s}
 
-    line = None
     if rank == 0:
         peaks = measured_peaks(torch)
-        peak = peaks["fp64_tflops_dgemm"]
-        flops = attempts_per_frame * F_ATTEMPT
-        achieved = flops / (ms * 1e-3) / 1e12
-        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (best of 5); MEASURED_PEAKS.json "
-                               "has no FP64 figure",
-                "flops_per_launch": flops, "flop_count": f"{F_ATTEMPT} per DP45 attempt x {attempts_per_frame} "
-                                                        f"attempts (device counter)",
-                "traffic": None, "kernel": "thin_render_kernel<0>"}
+        p64 = peaks["fp64_tflops_dgemm"]
+        p32 = sgemm_peak(torch)
+        forms = {}
+        for name, form in (("fp64", G.FORM_FP64), ("mixed", G.FORM_MIXED)):
+            r = res[form]
+            st = r["stats"]
+            forms[name] = {"value": world * RAYS / (r["ms"] * 1e-3), "unit": "rays/s", "ms_per_step": r["ms"],
+                           "phase_ms": r["phase_ms"], "attempts_per_ray": st["attempts"] / RAYS,
+                           "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])}
+        # FP64 form: thin_render_kernel, FP64 FLOPs against the DGEMM peak
+        st64 = res[G.FORM_FP64]["stats"]
+        fl64 = st64["attempts"] * F_ATTEMPT
+        a64 = fl64 / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
+        forms["fp64"]["roofline"] = {"kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": a64,
+                                     "peak": p64, "unit": "TFLOP/s", "frac": a64 / p64}
+        # mixed form: the speculation kernel (FP32 FLOPs vs the SGEMM peak) and
+        # the re-trace kernel (FP64 FLOPs vs the DGEMM peak)
+        stm = res[G.FORM_MIXED]["stats"]
+        ph = res[G.FORM_MIXED]["phase_ms"]
+        spec_att = stm["attempts"] - stm["fp64_attempts"]
+        a_spec = spec_att * F_ATTEMPT / (ph[0] * 1e-3) / 1e12
+        a_re = stm["fp64_attempts"] * F_ATTEMPT / (ph[2] * 1e-3) / 1e12
+        forms["mixed"]["phases"] = ["mixed_speculate_kernel", "mixed_star_kernel", "mixed_retrace_kernel",
+                                    "mixed_resolve_kernel"]
+        forms["mixed"]["roofline"] = {
+            "speculate": {"bound": "fp32", "achieved": a_spec, "peak": p32, "unit": "TFLOP/s", "frac": a_spec / p32},
+            "retrace": {"bound": "fp64", "achieved": a_re, "peak": p64, "unit": "TFLOP/s", "frac": a_re / p64}}
+        if head_form == G.FORM_MIXED:
+            roof = dict(forms["mixed"]["roofline"]["speculate"])
+            roof.update(kernel="mixed_speculate_kernel", flops_per_launch=spec_att * F_ATTEMPT,
+                        flop_count=f"{F_ATTEMPT} per DP45 attempt (FP32 stages) x {spec_att} speculative attempts "
+                                   f"(device counter)",
+                        peak_source="cuBLAS SGEMM 8192^3, TF32 off, measured in this run (best of 5); "
+                                    "MEASURED_PEAKS.json has no FP32 figure",
+                        launch_ms=ph[0], traffic=None)
+            launches = args.steps * (4 if params["background_type"] == G.BG_STARS else 3)
+        else:
+            roof = dict(forms["fp64"]["roofline"])
+            roof.update(flops_per_launch=fl64, flop_count=f"{F_ATTEMPT} per DP45 attempt x {st64['attempts']} "
+                                                          f"attempts (device counter)",
+                        peak_source="cuBLAS FP64 GEMM 8192^3 measured in this run (best of 5); MEASURED_PEAKS.json "
+                                    "has no FP64 figure", traffic=None)
+            launches = args.steps
+        err = form_error(torch, G, params)
         cpu = None
         if not args.no_cpu_baseline:
             try:
@@ -381,16 +478,20 @@ def main():
                        "sample": f"unavailable: {ex}"}
         line = {"metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if form == G.FORM_FP64 else "f32+f64",
+                "vs_baseline": None, "dtype": "f64" if head_form == G.FORM_FP64 else "f32+f64",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "rays_per_step": RAYS,
                            "form": args.form, "l2": "flushed between steps (256 MiB write)",
                            "parallelism": f"one frame per GPU per step ({world} GPU)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-                "gpu_launches": args.steps,
-                "work": {"attempts_per_ray": attempts_per_frame / RAYS, "accepted_per_ray": st["accepted"] / RAYS,
-                         "crossings": st["crossings"], "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])},
-                "kernel_ms_per_step": kernel_ms, "wall_s_timed_region": wall}
+                "gpu_launches": launches, "forms": forms,
+                "speedup_mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
+                "mixed_error_vs_fp64": err,
+                "work": {"attempts_per_ray": head["stats"]["attempts"] / RAYS,
+                         "accepted_per_ray": head["stats"]["accepted"] / RAYS,
+                         "crossings": head["stats"]["crossings"],
+                         "fp64_attempt_share": head["stats"]["fp64_attempts"] / max(1, head["stats"]["attempts"])},
+                "kernel_ms_per_step": head["kernel_ms"], "wall_s_timed_region": head["wall"]}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

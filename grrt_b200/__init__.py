@@ -120,6 +120,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
+        "grrt_get_phase_ms": (C.c_int, [vp, P(C.c_double), C.c_int]),
         "grrt_batch_create": (vp, [P(GRRTParams), C.c_int]),
         "grrt_batch_destroy": (None, [vp]),
         "grrt_batch_error": (C.c_char_p, [vp]),
@@ -310,6 +311,15 @@ class Renderer:
         st = GRRTStats()
         self._check(self._L.grrt_get_stats(self.ctx, C.byref(st)), "grrt_get_stats")
         return st.as_dict()
+
+    def phase_ms(self) -> list:
+        """Device time of each kernel phase of the last render (ms)."""
+        out = np.zeros(8, dtype=np.float64)
+        n = self._L.grrt_get_phase_ms(self.ctx, _dptr(out), 8)
+        if n < 0:
+            err = self._L.grrt_error(self.ctx)
+            raise RuntimeError("grrt_get_phase_ms failed: " + (err.decode() if err else f"rc={n}"))
+        return [float(x) for x in out[:n]]
 
     def table(self, name: str) -> np.ndarray:
         n = self._L.grrt_scene_table(self.ctx, name.encode(), None, 0)

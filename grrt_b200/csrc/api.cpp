@@ -263,7 +263,10 @@ extern "C" GRRT_EXPORT int grrt_set_precision(GRRTContext* ctx, int form) {
 extern "C" GRRT_EXPORT int grrt_get_precision(const GRRTContext* ctx) { return ctx ? ctx->form : -1; }
 
 extern "C" GRRT_EXPORT int grrt_set_mixed_params(GRRTContext* ctx, double r_factor, double tol_fp32) {
-    if (!ctx || !(r_factor >= 0.0) || !(tol_fp32 > 0.0)) return -1;
+    // r_near below the horizon would switch the near-critical test off; an FP32
+    // tolerance outside [1e-9, 1e-2] is below its error estimate's noise floor
+    // or too coarse for the speculative trajectory to be trusted
+    if (!ctx || !(r_factor >= 1.0 && r_factor <= 100.0) || !(tol_fp32 >= 1e-9 && tol_fp32 <= 1e-2)) return -1;
     ctx->mixed_r_factor = r_factor;
     ctx->tol_fp32 = tol_fp32;
     return 0;
@@ -292,6 +295,11 @@ extern "C" GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double*
 extern "C" GRRT_EXPORT int grrt_get_stats(GRRTContext* ctx, GRRTStats* out) {
     if (!ctx || !out) return -1;
     return ctx->read_stats(out);
+}
+
+extern "C" GRRT_EXPORT int grrt_get_phase_ms(GRRTContext* ctx, double* out, int capacity) {
+    if (!ctx || (!out && capacity > 0) || capacity < 0) return -1;
+    return ctx->phase_ms(out, capacity);
 }
 
 extern "C" GRRT_EXPORT long long grrt_scene_table(const GRRTContext* ctx, const char* name, double* out,

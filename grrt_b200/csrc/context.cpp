@@ -52,6 +52,8 @@ GRRTContext::~GRRTContext() {
         if (h_cancel) cudaFreeHost(h_cancel);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (cudaEvent_t& e : ev_phase)
+            if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
         cudaSetDevice(prev);
     }
@@ -273,6 +275,8 @@ bool GRRTContext::ensure_device() {
     if (fail_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
     if (fail_cuda(cudaEventCreate(&ev0), "cudaEventCreate")) return false;
     if (fail_cuda(cudaEventCreate(&ev1), "cudaEventCreate")) return false;
+    for (cudaEvent_t& e : ev_phase)
+        if (fail_cuda(cudaEventCreate(&e), "cudaEventCreate")) return false;
     device_ready = true;
     return true;
 }
@@ -329,16 +333,18 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
             d_mixed_scratch_bytes = mixed_bytes;
         }
     }
-    cudaEventRecord(ev0, s);
+    n_phases = 0;
+        cudaEventRecord(ev0, s);
     cudaError_t e;
     if (vol)
         e = launch_volume_rgb(S, tile, out, res, form, s);
     else if (mixed_thin)
         e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
-                              mixed_r_factor * r_horizon, s);
+                              mixed_r_factor * r_horizon, ev_phase, s);
     else
         e = launch_thin(S, tile, out, res, form, s);
     cudaEventRecord(ev1, s);
+    n_phases = mixed_thin ? kMixedPhases : 0;
     if (fail_cuda(e, "render launch")) return -1;
     return 0;
 }
@@ -403,6 +409,7 @@ int GRRTContext::render_spectral_device(int width, int height, double* d_spec, u
     if (!vol) {
         // No volumetric disk: the reference returns all-zero spectra
         // (src/geodesic_tracer.cpp:503-505).
+        n_phases = 0;
         cudaEventRecord(ev0, s);
         cudaError_t e = cudaMemsetAsync(d_spec, 0, n * sizeof(double), s);
         if (d_fate && e == cudaSuccess) {
@@ -450,7 +457,8 @@ int GRRTContext::render_spectral_device(int width, int height, double* d_spec, u
     out.spec = d_spec;
     out.fate = d_fate;
     const DevScene S = scene_for_launch();
-    cudaEventRecord(ev0, s);
+    n_phases = 0;
+        cudaEventRecord(ev0, s);
     cudaError_t e = launch_volume_spectral(S, tile, d_freqs, nb, out, res, form, s);
     cudaEventRecord(ev1, s);
     return fail_cuda(e, "spectral launch") ? -1 : 0;
@@ -537,6 +545,24 @@ int GRRTContext::read_stats(GRRTStats* out) {
     if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) out->kernel_ms = ms;
     cudaGetLastError();
     return 0;
+}
+
+int GRRTContext::phase_ms(double* out, int cap) {
+    if (!device_ready) return 0;
+    cudaSetDevice(device);
+    if (fail_cuda(cudaEventSynchronize(ev1), "synchronize")) return -1;
+    const int n = n_phases > 0 ? n_phases : 1;
+    for (int k = 0; k < n && k < cap; ++k) {
+        float ms = 0.0f;
+        const cudaError_t e = n_phases > 0 ? cudaEventElapsedTime(&ms, ev_phase[k], ev_phase[k + 1])
+                                           : cudaEventElapsedTime(&ms, ev0, ev1);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ms = 0.0f;
+        }
+        out[k] = ms;
+    }
+    return n;
 }
 
 bool GRRTContext::export_table(const std::string& name, std::vector<double>& v) const {

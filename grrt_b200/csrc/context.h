@@ -52,6 +52,10 @@ struct GRRTContext {
     int* d_cancel = nullptr;   // its device alias
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // per-kernel phases of the last render (mixed form: speculate, stars,
+    // re-trace, resolve; otherwise the one render kernel)
+    cudaEvent_t ev_phase[grrt_b200::kMixedPhases + 1] = {};
+    int n_phases = 0;
     double last_kernel_ms = 0.0;
     // cached device outputs for the host-buffer entry points
     void* d_out = nullptr;
@@ -80,6 +84,7 @@ struct GRRTContext {
     int render_spectral_to_host(int width, int height, double* host, grrt_progress_fn cb, void* user);
     int render_spectral_to_fits(const char* path, int width, int height, grrt_progress_fn cb, void* user);
     int read_stats(GRRTStats* out);
+    int phase_ms(double* out, int cap);
     bool export_table(const std::string& name, std::vector<double>& out) const;
     void debug_pixel(int px, int py);
     void request_cancel();

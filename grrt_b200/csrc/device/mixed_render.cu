@@ -44,55 +44,6 @@ __device__ __forceinline__ void sample_start(const DevScene& S, const DevTile& t
     pph = p[3];
 }
 
-// True when the star lookup at any point of the arc could find a star: one
-// scan of the cells every lookup along it can reach (the arc's cell span plus
-// the lookup's one-cell border), with a point-to-segment distance per star
-// against the lookup tolerance plus 1e-4 rad of slack (far-field model and
-// FP32 trajectory). Arcs near a pole, where the picture and the cell scan
-// break down, count as in reach.
-__device__ bool star_in_reach(const DevStars& st, const mixed::EscapeArc& e) {
-    double th0 = e.th0, ph0 = e.ph0;
-    double th1 = e.th0 + e.dth, ph1 = e.ph0 + e.dph;
-    const bool f0 = mixed::fold_sky(th0, ph0), f1 = mixed::fold_sky(th1, ph1);
-    constexpr double kCell = kPiD / 180.0;  // star grid cells are 1 degree
-    if (f0 != f1 || fmin(th0, th1) < 3.0 * kCell || fmax(th0, th1) > kPiD - 3.0 * kCell) return true;
-    double dph = ph1 - ph0;
-    if (dph > kPiD) dph -= 2.0 * kPiD;
-    if (dph < -kPiD) dph += 2.0 * kPiD;
-    if (fabs(dph) > 10.0 * kCell || fabs(th1 - th0) > 10.0 * kCell) return true;
-    // the lookup's distance metric weighs phi by sin(theta): take its smallest
-    // value along the segment (sin is concave on [0, pi])
-    const double s = fmin(sin(th0), sin(th1));
-    const double tol = sqrt(st.tol2) + 1e-4;
-    const double ex = th1 - th0, ey = dph * s;
-    const double e2 = ex * ex + ey * ey;
-    constexpr int nt = 180, np = 360;
-    const int t_lo = max(static_cast<int>(fmin(th0, th1) * nt / kPiD) - 1, 0);
-    const int t_hi = min(static_cast<int>(fmax(th0, th1) * nt / kPiD) + 1, nt - 1);
-    const double pa = fmin(ph0, ph0 + dph), pb = fmax(ph0, ph0 + dph);
-    const int p_lo = static_cast<int>(floor((pa + kPiD) * np / (2.0 * kPiD))) - 1;
-    const int p_hi = static_cast<int>(floor((pb + kPiD) * np / (2.0 * kPiD))) + 1;
-    for (int t = t_lo; t <= t_hi; ++t) {
-        for (int pc = p_lo; pc <= p_hi; ++pc) {
-            const int cell = t * np + ((pc % np) + np) % np;
-            const int q1 = __ldg(st.cell_start + cell + 1);
-            for (int q = __ldg(st.cell_start + cell); q < q1; ++q) {
-                const int si = __ldg(st.cell_items + q);
-                const double qx = __ldg(st.theta + si) - th0;
-                double qp = __ldg(st.phi + si) - ph0;
-                if (qp > kPiD) qp -= 2.0 * kPiD;
-                if (qp < -kPiD) qp += 2.0 * kPiD;
-                const double qy = qp * s;
-                double t_seg = e2 > 0.0 ? (qx * ex + qy * ey) / e2 : 0.0;
-                t_seg = fmin(fmax(t_seg, 0.0), 1.0);
-                const double dx = qx - t_seg * ex, dy = qy - t_seg * ey;
-                if (dx * dx + dy * dy < tol * tol) return true;
-            }
-        }
-    }
-    return false;
-}
-
 // Queues sample q for the FP64 re-trace (warp-aggregated over the lanes that ask).
 __device__ __forceinline__ void queue_retrace(bool want, unsigned q, const DevMixedBuffers& mb) {
     const int lane = threadIdx.x & 31;
@@ -243,7 +194,7 @@ mixed_star_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMix
             const double packed = mb.sample_rgb[o + 2];
             e.dth = __int_as_float(__double2hiint(packed));
             e.dph = __int_as_float(__double2loint(packed));
-            if (star_in_reach(S.stars, e)) {
+            if (mixed::star_in_reach(S.stars, e)) {
                 queue = true;
             } else {
                 mb.sample_rgb[o + 0] = 0.0;
@@ -394,7 +345,10 @@ size_t mixed_scratch_bytes(const DevTile& tile, int g2) {
 
 cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                               const LaunchResources& res, void* scratch, size_t scratch_bytes, double margin,
-                              double r_near, cudaStream_t stream) {
+                              double r_near, cudaEvent_t* phase_events, cudaStream_t stream) {
+    auto mark = [&](int k) {
+        if (phase_events) cudaEventRecord(phase_events[k], stream);
+    };
     DevStats* stats = res.stats;
     const int g2 = S.grid * S.grid;
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
@@ -425,9 +379,11 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
         if (per2 < 1) per2 = 1;
     }
     const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
+    mark(0);
     mixed_speculate_kernel<<<need < sms * per1 ? need : sms * per1, kMixThreads, 0, stream>>>(S, tile, mb, stats);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    mark(1);
     if (S.stars_on) {
         int sb = static_cast<int>((n + 255) / 256);
         if (sb > sms * 8) sb = sms * 8;
@@ -435,14 +391,18 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
+    mark(2);
     mixed_retrace_kernel<<<sms * per2, kMixThreads, 0, stream>>>(S, tile, mb, stats);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    mark(3);
     const size_t npix = static_cast<size_t>(tile.w) * tile.h;
     int rb = static_cast<int>((npix + 255) / 256);
     if (rb > sms * 8) rb = sms * 8;
     mixed_resolve_kernel<<<rb, 256, 0, stream>>>(S, tile, mb, out.rgba, out.rgb64, out.fate, stats);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    mark(4);
+    return e;
 }
 
 }  // namespace grrt_b200

@@ -21,6 +21,13 @@
 #pragma once
 
 #include "integrate.cuh"
+#include "scene.h"
+
+#ifdef __CUDA_ARCH__
+#define GRRT_LDG(p) __ldg(p)
+#else
+#define GRRT_LDG(p) (*(p))
+#endif
 
 namespace grrt_b200 {
 namespace mixed {
@@ -117,6 +124,58 @@ GRRT_HD bool fold_sky(double& theta, double& phi) {
     if (phi > kPi) phi -= 2.0 * kPi;
     if (phi < -kPi) phi += 2.0 * kPi;
     return flip;
+}
+
+GRRT_HD int imax(int a, int b) { return a > b ? a : b; }
+GRRT_HD int imin(int a, int b) { return a < b ? a : b; }
+
+// True when the star lookup at any point of the arc could find a star: one
+// scan of the cells every lookup along it can reach (the arc's cell span plus
+// the lookup's one-cell border), with a point-to-segment distance per star
+// against the lookup tolerance plus 1e-4 rad of slack (far-field model and
+// FP32 trajectory). Arcs near a pole, where the picture and the cell scan
+// break down, count as in reach.
+GRRT_HD bool star_in_reach(const DevStars& st, const mixed::EscapeArc& e) {
+    double th0 = e.th0, ph0 = e.ph0;
+    double th1 = e.th0 + e.dth, ph1 = e.ph0 + e.dph;
+    const bool f0 = mixed::fold_sky(th0, ph0), f1 = mixed::fold_sky(th1, ph1);
+    constexpr double kCell = kPi / 180.0;  // star grid cells are 1 degree
+    if (f0 != f1 || fmin(th0, th1) < 3.0 * kCell || fmax(th0, th1) > kPi - 3.0 * kCell) return true;
+    double dph = ph1 - ph0;
+    if (dph > kPi) dph -= 2.0 * kPi;
+    if (dph < -kPi) dph += 2.0 * kPi;
+    if (fabs(dph) > 10.0 * kCell || fabs(th1 - th0) > 10.0 * kCell) return true;
+    // the lookup's distance metric weighs phi by sin(theta): take its smallest
+    // value along the segment (sin is concave on [0, pi])
+    const double s = fmin(sin(th0), sin(th1));
+    const double tol = sqrt(st.tol2) + 1e-4;
+    const double ex = th1 - th0, ey = dph * s;
+    const double e2 = ex * ex + ey * ey;
+    constexpr int nt = 180, np = 360;
+    const int t_lo = imax(static_cast<int>(fmin(th0, th1) * nt / kPi) - 1, 0);
+    const int t_hi = imin(static_cast<int>(fmax(th0, th1) * nt / kPi) + 1, nt - 1);
+    const double pa = fmin(ph0, ph0 + dph), pb = fmax(ph0, ph0 + dph);
+    const int p_lo = static_cast<int>(floor((pa + kPi) * np / (2.0 * kPi))) - 1;
+    const int p_hi = static_cast<int>(floor((pb + kPi) * np / (2.0 * kPi))) + 1;
+    for (int t = t_lo; t <= t_hi; ++t) {
+        for (int pc = p_lo; pc <= p_hi; ++pc) {
+            const int cell = t * np + ((pc % np) + np) % np;
+            const int q1 = GRRT_LDG(st.cell_start + cell + 1);
+            for (int q = GRRT_LDG(st.cell_start + cell); q < q1; ++q) {
+                const int si = GRRT_LDG(st.cell_items + q);
+                const double qx = GRRT_LDG(st.theta + si) - th0;
+                double qp = GRRT_LDG(st.phi + si) - ph0;
+                if (qp > kPi) qp -= 2.0 * kPi;
+                if (qp < -kPi) qp += 2.0 * kPi;
+                const double qy = qp * s;
+                double t_seg = e2 > 0.0 ? (qx * ex + qy * ey) / e2 : 0.0;
+                t_seg = fmin(fmax(t_seg, 0.0), 1.0);
+                const double dx = qx - t_seg * ex, dy = qy - t_seg * ey;
+                if (dx * dx + dy * dy < tol * tol) return true;
+            }
+        }
+    }
+    return false;
 }
 
 }  // namespace mixed

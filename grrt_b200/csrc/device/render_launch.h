@@ -58,9 +58,12 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
 
 // Mixed-precision thin-disk render: FP32 speculation, FP64 re-trace, resolve.
 size_t mixed_scratch_bytes(const DevTile& tile, int g2);
+// phase_events: NULL, or kMixedPhases + 1 events recorded on the stream around
+// the phases (speculate, stars, re-trace, resolve).
+constexpr int kMixedPhases = 4;
 cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                               const LaunchResources& res, void* scratch, size_t scratch_bytes, double margin,
-                              double r_near, cudaStream_t stream);
+                              double r_near, cudaEvent_t* phase_events, cudaStream_t stream);
 
 // Batched thin-disk render over many cameras (see DevBatch).
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,

@@ -21,8 +21,12 @@ extern "C" {
 #endif
 
 /* Precision forms. FP64: the reference method (Dormand-Prince 5(4) + PI
- * control, src/rk4.cpp:87-136) in double throughout. MIXED: FP32 right-hand
- * sides while the ray is far from the hole, FP64 state and FP64 near it. */
+ * control, src/rk4.cpp:87-136) in double throughout. MIXED, thin disk: every
+ * sample is integrated first with FP32 right-hand sides (FP64 state); samples
+ * whose colour depends on the FP64 step sequence (emitting crossings, grazes,
+ * near-critical orbits, escapes with a star in reach, the step budget) are
+ * re-traced with the FP64 method, all others are exactly 0. MIXED, volumetric
+ * disk: FP32 right-hand sides while the ray is far from the hole. */
 #define GRRT_FORM_FP64 0
 #define GRRT_FORM_MIXED 1
 
@@ -48,9 +52,19 @@ typedef struct {
 GRRT_EXPORT int grrt_set_precision(GRRTContext* ctx, int form);
 GRRT_EXPORT int grrt_get_precision(const GRRTContext* ctx);
 
-/* Mixed-form knobs: outer steps that start at r > r_factor * r_horizon use
- * FP32 right-hand sides controlled against tol_fp32; defaults 3.0 and 1e-6. */
+/* Mixed-form knobs. Thin disk: every sample is first integrated with FP32
+ * right-hand sides against tol_fp32; a sample that sweeps more than 3 rad
+ * inside r_factor * r_horizon (near-critical) is among those re-traced in FP64.
+ * Volumetric disk: outer steps that start at r > r_factor * r_horizon use FP32
+ * right-hand sides against tol_fp32. Defaults 3.0 and 1e-6; r_factor must lie
+ * in [1, 100] and tol_fp32 in [1e-9, 1e-2], else -1. */
 GRRT_EXPORT int grrt_set_mixed_params(GRRTContext* ctx, double r_factor, double tol_fp32);
+
+/* Device time (ms, CUDA events on the render stream) of each kernel phase of
+ * the last render: the mixed thin-disk form has 4 (FP32 speculation, star
+ * pass, FP64 re-trace, resolve); every other render has 1. Writes at most
+ * capacity values; returns the number of phases, or -1. Waits for the render. */
+GRRT_EXPORT int grrt_get_phase_ms(GRRTContext* ctx, double* out, int capacity);
 
 /* RGB render into device memory (the loop of Renderer::render,
  * src/renderer.cpp:30-82). d_rgba: float[W*H*4] or NULL; d_rgb64: the

@@ -1,6 +1,7 @@
 // Host build of the device math headers, so CPU tests can check the kernels'
 // right-hand side and integrator step against the oracle. Test-only.
 #include "../../grrt_b200/csrc/device/integrate.cuh"
+#include "../../grrt_b200/csrc/device/mixed_spec.cuh"
 
 using namespace grrt_b200;
 
@@ -28,4 +29,55 @@ double devmath_dp45(double M, double a, const double* y8, double h, double* out5
     return err;
 }
 
+
+// The mixed form's speculative pass for one sample, as mixed_speculate_kernel
+// and mixed_star_kernel run it. sc = (M, a, r_stop, r_escape, dl0, tol_fp32,
+// max_steps, r_in, r_out, margin, r_near, disk_on, stars_on); star arrays may
+// be null when stars_on is 0. Returns 1 when the sample goes to the FP64
+// re-trace, 0 when its colour is final (exactly 0); *term_out = the
+// speculative termination (-1 when it stopped early for the re-trace).
+int devmath_speculate(const double* sc, const double* y8, const double* st_th, const double* st_ph,
+                      const int* cells, const int* items, double tol2, int* term_out) {
+    const double M = sc[0], a = sc[1], r_stop = sc[2], r_esc = sc[3], dl0 = sc[4], tol32 = sc[5];
+    const int max_steps = static_cast<int>(sc[6]);
+    const bool disk_on = sc[11] != 0.0, stars_on = sc[12] != 0.0;
+    const double pt = y8[4], pph = y8[7];
+    Vec5<double> y{y8[1], y8[2], y8[3], y8[5], y8[6]};
+    double dl = dl0;
+    int retry = 0, step = 0;
+    mixed::Tracker trk;
+    trk.reset(disk_on, sc[7], sc[8], sc[9], sc[10]);
+    Vec5<float> k7{};
+    *term_out = -1;
+    while (true) {
+        if (retry == 0) {
+            if (step >= max_steps) { *term_out = kTermMaxSteps; return 1; }
+            if (y.r < r_stop) { *term_out = kTermHorizon; return 0; }
+            if (y.r > r_esc) break;
+        }
+        Vec5<double> y5;
+        const double err = mixed_attempt_impl(float(M), float(a), float(pt), float(pph), y, dl, y5, k7);
+        const StepDecision d = pi_control(err, tol32, dl, retry, y5.r);
+        if (d.accept) {
+            const bool hit = trk.step(y, y5);
+            y = y5;
+            if (hit) return 1;
+            dl = d.next;
+            retry = 0;
+            ++step;
+        } else {
+            dl = d.next;
+            ++retry;
+        }
+    }
+    *term_out = kTermEscaped;
+    if (!stars_on) return 0;
+    DevStars st;
+    st.theta = st_th;
+    st.phi = st_ph;
+    st.cell_start = cells;
+    st.cell_items = items;
+    st.tol2 = tol2;
+    return mixed::star_in_reach(st, mixed::escape_arc(r_esc, y, k7)) ? 1 : 0;
+}
 }

@@ -1,0 +1,82 @@
+"""The mixed form's speculative pass (grrt_b200/csrc/device/mixed_spec.cuh),
+compiled as host code, against the oracle. CPU only.
+
+The mixed form keeps a speculative FP32 result only when it is exactly 0
+(horizon, or escape with no star within reach of the lookup); everything else
+is re-traced with the FP64 method. So the bar is one-sided and exact: every
+sample whose oracle colour is non-zero, or that crosses the disk inside
+[r_in, r_out], must be sent to the re-trace. The flagged fraction is bounded
+too, so a pass that re-traces everything cannot meet the bar.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from oracle_bind import Oracle, jittered_samples
+from test_device_math import devmath  # noqa: F401  (fixture)
+
+STAR_TOL = 0.003  # the star catalogue's angular tolerance (rad)
+
+
+def speculate_all(L, R, px, py, margin=0.05, r_factor=3.0, tol32=1e-6):
+    sc = R.table("scalars")
+    M, a, rh, isco, robs, _tol, max_steps = sc[:7]
+    disk = R.values["disk_enabled"] != 0
+    r_in, r_out = (R.table("flux_meta")[1], R.table("flux_meta")[2]) if disk else (0.0, 0.0)
+    stars = R.values["background_type"] == 1
+    v = np.array([M, a, rh + 0.01, 1000.0, 0.01 * robs, tol32, max_steps, r_in, r_out, margin, r_factor * rh,
+                  1.0 if disk else 0.0, 1.0 if stars else 0.0])
+    PD, PI = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    hold = []
+    if stars:
+        st = R.table("stars").reshape(-1, 3)
+        th, ph = np.ascontiguousarray(st[:, 0]), np.ascontiguousarray(st[:, 1])
+        cells = R.table("star_cells").astype(np.int32)
+        items = R.table("star_items").astype(np.int32)
+        hold = [th, ph, cells, items]
+        args = (th.ctypes.data_as(PD), ph.ctypes.data_as(PD), cells.ctypes.data_as(PI), items.ctypes.data_as(PI))
+    else:
+        args = (None, None, None, None)
+    O = Oracle(R)
+    flags = np.zeros(len(px), dtype=np.int32)
+    terms = np.zeros(len(px), dtype=np.int32)
+    t = C.c_int()
+    for k, (x, y) in enumerate(zip(px, py)):
+        y8 = O.camera_ray(x, y)
+        flags[k] = L.devmath_speculate(v.ctypes.data_as(PD), y8.ctypes.data_as(PD), *args, STAR_TOL ** 2,
+                                       C.byref(t))
+        terms[k] = t.value
+    del hold
+    return flags, terms
+
+
+CASES = [
+    ("schwarzschild 80deg", 1, 72, {}),
+    ("kerr 0.998 80deg stars", 2, 56, {}),
+    ("kerr 0.998 edge-on stars", 2, 56, {"observer_theta": math.pi / 2}),
+    ("kerr 0.5 30deg stars", 2, 48, {"spin": 0.5, "observer_theta": math.radians(30.0)}),
+]
+
+
+@pytest.mark.parametrize("name,cfg,n,kw", CASES, ids=[c[0] for c in CASES])
+def test_speculation_flags_every_sample_with_colour(grrt, devmath, name, cfg, n, kw):  # noqa: F811
+    L = devmath
+    L.devmath_speculate.restype = C.c_int
+    L.devmath_speculate.argtypes = [C.POINTER(C.c_double)] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_double,
+                                                                                            C.POINTER(C.c_int)]
+    R = grrt.Renderer(grrt.config_params(cfg, width=n, height=n, spp=1, **kw))
+    px, py = jittered_samples(n, n, 1, np.arange(n * n))
+    flags, terms = speculate_all(L, R, px, py)
+    O = Oracle(R)
+    rgb, term, ncross, _fin, _cnt = O.trace_rgb(px, py)
+    coloured = np.any(rgb != 0.0, axis=1) | (ncross > 0) | (term == 2)
+    missed = np.nonzero(coloured & (flags == 0))[0]
+    assert len(missed) == 0, f"{name}: {len(missed)} samples with colour kept as 0, e.g. {missed[:5]}"
+    # a final speculative zero keeps the oracle's termination
+    keep = flags == 0
+    assert np.all(terms[keep] == term[keep]), f"{name}: termination differs on kept samples"
+    frac = flags.mean()
+    print(f"\n  [{name}] flagged {frac:.3f} of samples; coloured {coloured.mean():.3f}")
+    assert frac <= max(0.5, 1.6 * coloured.mean())
