@@ -121,6 +121,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
         "grrt_get_phase_ms": (C.c_int, [vp, P(C.c_double), C.c_int]),
+        "grrt_surrogate_gemm_bf16": (C.c_int, [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp,
+                                               C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp]),
         "grrt_batch_create": (vp, [P(GRRTParams), C.c_int]),
         "grrt_batch_destroy": (None, [vp]),
         "grrt_batch_error": (C.c_char_p, [vp]),
