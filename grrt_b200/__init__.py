@@ -21,7 +21,7 @@ import numpy as np
 
 __all__ = [
     "GRRTParams", "GRRTStats", "Renderer", "lib", "load_library", "build",
-    "FORM_FP64", "FORM_MIXED", "config_params", "LIB_PATH",
+    "FORM_FP64", "FORM_MIXED", "config_params", "LIB_PATH", "Surrogate",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -121,6 +121,25 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
         "grrt_get_phase_ms": (C.c_int, [vp, P(C.c_double), C.c_int]),
+        "grrt_surrogate_create": (vp, [C.c_uint]),
+        "grrt_surrogate_destroy": (None, [vp]),
+        "grrt_surrogate_error": (C.c_char_p, [vp]),
+        "grrt_surrogate_generate": (C.c_int, [vp, vp, C.c_int, C.c_int]),
+        "grrt_surrogate_dataset": (C.c_longlong, [vp, P(C.c_float), P(C.c_float), C.c_longlong]),
+        "grrt_surrogate_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_double, P(C.c_float)]),
+        "grrt_surrogate_calibrate": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, P(C.c_double)]),
+        "grrt_surrogate_set_bands": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
+        "grrt_surrogate_get_bands": (C.c_int, [vp, P(C.c_double)]),
+        "grrt_surrogate_params": (C.c_longlong, [vp, P(C.c_float), C.c_longlong]),
+        "grrt_surrogate_set_params": (C.c_int, [vp, P(C.c_float), C.c_longlong]),
+        "grrt_surrogate_forward": (C.c_int, [vp, vp, C.c_longlong, vp]),
+        "grrt_surrogate_gradients": (C.c_int, [vp, P(C.c_float), P(C.c_float), C.c_int, P(C.c_float),
+                                               P(C.c_double)]),
+        "grrt_surrogate_render_device": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+        "grrt_surrogate_render": (C.c_int, [vp, vp, P(C.c_float)]),
+        "grrt_surrogate_last_exact": (C.c_int, [vp, P(C.c_longlong), P(C.c_longlong)]),
+        "grrt_surrogate_save": (C.c_int, [vp, C.c_char_p]),
+        "grrt_surrogate_load": (C.c_int, [vp, C.c_char_p]),
         "grrt_surrogate_gemm_bf16": (C.c_int, [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp,
                                                C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp]),
         "grrt_batch_create": (vp, [P(GRRTParams), C.c_int]),
@@ -404,6 +423,132 @@ class Batch:
         st = GRRTStats()
         self._check(self._L.grrt_batch_get_stats(self.b, C.byref(st)), "grrt_batch_get_stats")
         return st.as_dict()
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Surrogate:
+    """The learned surrogate (include/grrt_surrogate.h): MLP 4 -> 256 x 4 -> 6,
+    trained on the GPU by the library's tensor-core kernels."""
+
+    N_PARAMS = 256 * 4 + 256 + 3 * (256 * 256 + 256) + 16 * 256 + 16
+    Y_COLS = 10
+
+    def __init__(self, seed: int = 0):
+        self._L = lib()
+        self.s = self._L.grrt_surrogate_create(seed)
+        if not self.s:
+            err = self._L.grrt_surrogate_error(None)
+            raise RuntimeError("grrt_surrogate_create failed: " + (err.decode() if err else "unknown"))
+
+    def close(self) -> None:
+        if getattr(self, "s", None):
+            self._L.grrt_surrogate_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            err = self._L.grrt_surrogate_error(self.s)
+            raise RuntimeError(f"{what} failed: " + (err.decode() if err else f"rc={rc}"))
+
+    @staticmethod
+    def _cams(cameras: Sequence[dict]):
+        arr = (GRRTParams * len(cameras))()
+        for i, c in enumerate(cameras):
+            arr[i] = make_params(c)
+        return arr
+
+    def generate(self, cameras: Sequence[dict], n_side: int) -> None:
+        arr = self._cams(cameras)
+        self._check(self._L.grrt_surrogate_generate(self.s, arr, len(cameras), n_side), "grrt_surrogate_generate")
+
+    def dataset(self):
+        n = self._L.grrt_surrogate_dataset(self.s, None, None, 0)
+        X = np.empty((n, 4), dtype=np.float32)
+        Y = np.empty((n, self.Y_COLS), dtype=np.float32)
+        if n:
+            self._L.grrt_surrogate_dataset(self.s, _fptr(X), _fptr(Y), n)
+        return X, Y
+
+    def train(self, steps: int, batch: int = 16384, lr: float = 1e-3) -> np.ndarray:
+        hist = np.empty(steps, dtype=np.float32)
+        self._check(self._L.grrt_surrogate_train(self.s, steps, batch, lr, _fptr(hist)), "grrt_surrogate_train")
+        return hist
+
+    def calibrate(self, cameras: Sequence[dict], n_side: int, quantile: float = 0.999, safety: float = 1.5) -> dict:
+        arr = self._cams(cameras)
+        rep = np.zeros(8)
+        self._check(self._L.grrt_surrogate_calibrate(self.s, arr, len(cameras), n_side, quantile, safety, _dptr(rep)),
+                    "grrt_surrogate_calibrate")
+        keys = ["du", "dir", "capture", "graze", "samples", "fate_disagreements", "band_fraction", "median_du"]
+        return dict(zip(keys, rep.tolist()))
+
+    def set_bands(self, du: float, dir: float, capture: float, graze: float, tol_rel: float = 1e-3) -> None:
+        self._check(self._L.grrt_surrogate_set_bands(self.s, du, dir, capture, graze, tol_rel),
+                    "grrt_surrogate_set_bands")
+
+    def bands(self) -> dict:
+        out = np.zeros(5)
+        self._L.grrt_surrogate_get_bands(self.s, _dptr(out))
+        return dict(zip(["du", "dir", "capture", "graze", "tol_rel"], out.tolist()))
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.N_PARAMS, dtype=np.float32)
+        n = self._L.grrt_surrogate_params(self.s, _fptr(p), self.N_PARAMS)
+        assert n == self.N_PARAMS
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self._L.grrt_surrogate_set_params(self.s, _fptr(p), len(p)), "grrt_surrogate_set_params")
+
+    def forward(self, d_in, d_out, n: int) -> None:
+        """Device pointers (int) or torch tensors: inputs float[n][4] -> outputs float[n][16]."""
+        pi = d_in if isinstance(d_in, int) else d_in.data_ptr()
+        po = d_out if isinstance(d_out, int) else d_out.data_ptr()
+        self._check(self._L.grrt_surrogate_forward(self.s, pi, n, po), "grrt_surrogate_forward")
+
+    def gradients(self, X: np.ndarray, Y: np.ndarray):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        g = np.empty(self.N_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        self._check(self._L.grrt_surrogate_gradients(self.s, _fptr(X), _fptr(Y), len(X), _fptr(g), C.byref(loss)),
+                    "grrt_surrogate_gradients")
+        return loss.value, g
+
+    def render_device(self, R: "Renderer", d_rgba=None, d_rgb64=None, d_fate=None, stream=None) -> None:
+        def ptr(x):
+            if x is None:
+                return None
+            return x if isinstance(x, int) else x.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        rc = self._L.grrt_surrogate_render_device(self.s, R.ctx, ptr(d_rgba), ptr(d_rgb64), ptr(d_fate), s)
+        self._check(rc, "grrt_surrogate_render_device")
+
+    def render(self, R: "Renderer") -> np.ndarray:
+        fb = np.empty((R.height, R.width, 4), dtype=np.float32)
+        self._check(self._L.grrt_surrogate_render(self.s, R.ctx, _fptr(fb)), "grrt_surrogate_render")
+        return fb
+
+    def last_exact(self):
+        e, n = C.c_longlong(), C.c_longlong()
+        self._L.grrt_surrogate_last_exact(self.s, C.byref(e), C.byref(n))
+        return e.value, n.value
+
+    def save(self, path: str) -> None:
+        self._check(self._L.grrt_surrogate_save(self.s, path.encode()), "grrt_surrogate_save")
+
+    def load(self, path: str) -> None:
+        self._check(self._L.grrt_surrogate_load(self.s, path.encode()), "grrt_surrogate_load")
 
 
 def sweep_cameras(width: int = 256, height: int = 256, spins=(0.0, 0.5, 0.9, 0.998), n_incl: int = 16,

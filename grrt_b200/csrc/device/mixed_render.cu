@@ -343,6 +343,55 @@ size_t mixed_scratch_bytes(const DevTile& tile, int g2) {
     return n * (3 * sizeof(double) + 2 * sizeof(unsigned)) + 1024;
 }
 
+namespace {
+struct MixLaunchShape {
+    int sms = 0, per_spec = 1, per_retrace = 1;
+};
+const MixLaunchShape& mix_shape() {
+    static MixLaunchShape sh;
+    if (sh.sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sh.sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, mixed_speculate_kernel, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, mixed_retrace_kernel, kMixThreads, 0);
+        if (sh.per_spec < 1) sh.per_spec = 1;
+        if (sh.per_retrace < 1) sh.per_retrace = 1;
+    }
+    return sh;
+}
+}  // namespace
+
+DevMixedBuffers mixed_buffers(void* scratch, size_t n, unsigned* queue) {
+    auto* base = static_cast<unsigned char*>(scratch);
+    DevMixedBuffers mb;
+    mb.queue = queue;
+    mb.queue2 = reinterpret_cast<unsigned*>(base + 256);
+    mb.retrace_count = reinterpret_cast<unsigned*>(base + 512);
+    mb.sample_rgb = reinterpret_cast<double*>(base + 1024);
+    mb.sample_fate = reinterpret_cast<uint32_t*>(base + 1024 + n * 3 * sizeof(double));
+    mb.retrace_list = mb.sample_fate + n;
+    return mb;
+}
+
+cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
+                                 cudaStream_t stream) {
+    const MixLaunchShape& sh = mix_shape();
+    mixed_retrace_kernel<<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, mb, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                                 const ThinOutputs& out, DevStats* stats, cudaStream_t stream) {
+    const MixLaunchShape& sh = mix_shape();
+    const size_t npix = static_cast<size_t>(tile.w) * tile.h;
+    int rb = static_cast<int>((npix + 255) / 256);
+    if (rb > sh.sms * 8) rb = sh.sms * 8;
+    if (rb < 1) rb = 1;
+    mixed_resolve_kernel<<<rb, 256, 0, stream>>>(S, tile, mb, out.rgba, out.rgb64, out.fate, stats);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                               const LaunchResources& res, void* scratch, size_t scratch_bytes, double margin,
                               double r_near, cudaEvent_t* phase_events, cudaStream_t stream) {
@@ -354,53 +403,34 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
     if (n == 0) return cudaSuccess;
     if (scratch_bytes < mixed_scratch_bytes(tile, g2)) return cudaErrorInvalidValue;
-    auto* base = static_cast<unsigned char*>(scratch);
-    DevMixedBuffers mb;
-    mb.queue = res.queue;  // the phase-1 counter doubles as the progress counter
-    mb.queue2 = reinterpret_cast<unsigned*>(base + 256);
-    mb.retrace_count = reinterpret_cast<unsigned*>(base + 512);
-    mb.sample_rgb = reinterpret_cast<double*>(base + 1024);
-    mb.sample_fate = reinterpret_cast<uint32_t*>(base + 1024 + n * 3 * sizeof(double));
-    mb.retrace_list = mb.sample_fate + n;
+    // the phase-1 counter doubles as the progress counter
+    DevMixedBuffers mb = mixed_buffers(scratch, n, res.queue);
     mb.margin = margin;
     mb.r_near = r_near;
-    cudaError_t e = cudaMemsetAsync(base, 0, 1024, stream);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 1024, stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
-    static int sms = 0, per1 = 0, per2 = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, mixed_speculate_kernel, kMixThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, mixed_retrace_kernel, kMixThreads, 0);
-        if (per1 < 1) per1 = 1;
-        if (per2 < 1) per2 = 1;
-    }
+    const MixLaunchShape& sh = mix_shape();
     const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
     mark(0);
-    mixed_speculate_kernel<<<need < sms * per1 ? need : sms * per1, kMixThreads, 0, stream>>>(S, tile, mb, stats);
+    mixed_speculate_kernel<<<need < sh.sms * sh.per_spec ? need : sh.sms * sh.per_spec, kMixThreads, 0, stream>>>(
+        S, tile, mb, stats);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     mark(1);
     if (S.stars_on) {
         int sb = static_cast<int>((n + 255) / 256);
-        if (sb > sms * 8) sb = sms * 8;
+        if (sb > sh.sms * 8) sb = sh.sms * 8;
         mixed_star_kernel<<<sb, 256, 0, stream>>>(S, tile, mb);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     mark(2);
-    mixed_retrace_kernel<<<sms * per2, kMixThreads, 0, stream>>>(S, tile, mb, stats);
-    e = cudaGetLastError();
+    e = launch_mixed_retrace(S, tile, mb, stats, stream);
     if (e != cudaSuccess) return e;
     mark(3);
-    const size_t npix = static_cast<size_t>(tile.w) * tile.h;
-    int rb = static_cast<int>((npix + 255) / 256);
-    if (rb > sms * 8) rb = sms * 8;
-    mixed_resolve_kernel<<<rb, 256, 0, stream>>>(S, tile, mb, out.rgba, out.rgb64, out.fate, stats);
-    e = cudaGetLastError();
+    e = launch_mixed_resolve(S, tile, mb, out, stats, stream);
     mark(4);
     return e;
 }

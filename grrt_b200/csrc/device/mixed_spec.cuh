@@ -132,10 +132,10 @@ GRRT_HD int imin(int a, int b) { return a < b ? a : b; }
 // True when the star lookup at any point of the arc could find a star: one
 // scan of the cells every lookup along it can reach (the arc's cell span plus
 // the lookup's one-cell border), with a point-to-segment distance per star
-// against the lookup tolerance plus 1e-4 rad of slack (far-field model and
-// FP32 trajectory). Arcs near a pole, where the picture and the cell scan
+// against the lookup tolerance plus `slack` rad (default 1e-4: far-field
+// model and FP32 trajectory). Arcs near a pole, where the picture and the cell scan
 // break down, count as in reach.
-GRRT_HD bool star_in_reach(const DevStars& st, const mixed::EscapeArc& e) {
+GRRT_HD bool star_in_reach(const DevStars& st, const mixed::EscapeArc& e, double slack = 1e-4) {
     double th0 = e.th0, ph0 = e.ph0;
     double th1 = e.th0 + e.dth, ph1 = e.ph0 + e.dph;
     const bool f0 = mixed::fold_sky(th0, ph0), f1 = mixed::fold_sky(th1, ph1);
@@ -148,7 +148,7 @@ GRRT_HD bool star_in_reach(const DevStars& st, const mixed::EscapeArc& e) {
     // the lookup's distance metric weighs phi by sin(theta): take its smallest
     // value along the segment (sin is concave on [0, pi])
     const double s = fmin(sin(th0), sin(th1));
-    const double tol = sqrt(st.tol2) + 1e-4;
+    const double tol = sqrt(st.tol2) + slack;
     const double ex = th1 - th0, ey = dph * s;
     const double e2 = ex * ex + ey * ey;
     constexpr int nt = 180, np = 360;

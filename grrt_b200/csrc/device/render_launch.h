@@ -65,6 +65,17 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
                               const LaunchResources& res, void* scratch, size_t scratch_bytes, double margin,
                               double r_near, cudaEvent_t* phase_events, cudaStream_t stream);
 
+// The mixed form's buffers inside a scratch of mixed_scratch_bytes (queue is
+// the caller's phase-1 counter), and its re-trace and resolve phases on their
+// own: the re-trace traces retrace_list[0 .. *retrace_count) with the FP64
+// method into sample_rgb / sample_fate; the resolve sums samples into pixels.
+// queue2 and retrace_count (scratch bytes 256..1023) must be zeroed first.
+DevMixedBuffers mixed_buffers(void* scratch, size_t n_samples, unsigned* queue);
+cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
+                                 cudaStream_t stream);
+cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                                 const ThinOutputs& out, DevStats* stats, cudaStream_t stream);
+
 // Batched thin-disk render over many cameras (see DevBatch).
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,
                               int blocks, cudaStream_t stream);

@@ -42,7 +42,7 @@ struct GemmSmem {
     int failed;
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
     const float s = 1.0f / (1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));

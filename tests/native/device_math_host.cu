@@ -2,6 +2,7 @@
 // right-hand side and integrator step against the oracle. Test-only.
 #include "../../grrt_b200/csrc/device/integrate.cuh"
 #include "../../grrt_b200/csrc/device/mixed_spec.cuh"
+#include "../../grrt_b200/csrc/device/surrogate_geom.cuh"
 
 using namespace grrt_b200;
 
@@ -79,5 +80,60 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
     st.cell_items = items;
     st.tol2 = tol2;
     return mixed::star_in_reach(st, mixed::escape_arc(r_esc, y, k7)) ? 1 : 0;
+}
+
+// Closed-form margins of the surrogate for a camera ray y8 = (t, r, th, ph,
+// p_t, p_r, p_th, p_ph): out2 = (capture margin, graze margin).
+void devmath_ray_margins(double M, double a, double r_h, const double* y8, double* out2) {
+    const double p[4] = {y8[4], y8[5], y8[6], y8[7]};
+    const surr::RayConstants k = surr::constants(a, y8[2], p);
+    out2[0] = (p[1] < 0.0) ? surr::capture_margin(M, a, k, r_h, y8[1]) : -1.0;
+    out2[1] = surr::graze_margin(a, k);
+}
+
+// The surrogate's training trace (the FP64 method, as the thin-disk kernel)
+// of one camera ray: sc = (M, a, r_stop, r_escape, dl0, tol, max_steps, r_cut)
+// with r_cut the smallest crossing radius recorded. out = (termination,
+// crossings outside r_cut, first and second such radius, accepted steps).
+void devmath_trace_crossings(const double* sc, const double* y8, double* out) {
+    const double M = sc[0], a = sc[1], r_stop = sc[2], r_esc = sc[3], dl0 = sc[4], tol = sc[5], r_cut = sc[7];
+    const int max_steps = static_cast<int>(sc[6]);
+    const double pt = y8[4], pph = y8[7];
+    Vec5<double> y{y8[1], y8[2], y8[3], y8[5], y8[6]};
+    double dl = dl0, r1 = 0.0, r2 = 0.0;
+    int retry = 0, step = 0, nc = 0, term = -1;
+    while (true) {
+        if (retry == 0) {
+            if (step >= max_steps) { term = kTermMaxSteps; break; }
+            if (y.r < r_stop) { term = kTermHorizon; break; }
+            if (y.r > r_esc) { term = kTermEscaped; break; }
+        }
+        Vec5<double> y5;
+        const double err = dp45_attempt<double>(M, a, pt, pph, y, dl, y5);
+        const StepDecision d = pi_control(err, tol, dl, retry, y5.r);
+        if (d.accept) {
+            const double dp = y.th - 0.5 * mixed::kPi, dn = y5.th - 0.5 * mixed::kPi;
+            if (dp * dn < 0.0 && fabs(dp - dn) > 1e-12) {
+                const double rc = y.r + (-dp / (dn - dp)) * (y5.r - y.r);
+                if (rc >= r_cut) {
+                    if (nc == 0) r1 = rc;
+                    else if (nc == 1) r2 = rc;
+                    ++nc;
+                }
+            }
+            y = y5;
+            dl = d.next;
+            retry = 0;
+            ++step;
+        } else {
+            dl = d.next;
+            ++retry;
+        }
+    }
+    out[0] = term;
+    out[1] = nc;
+    out[2] = r1;
+    out[3] = r2;
+    out[4] = step;
 }
 }

@@ -19,7 +19,7 @@ OUT = os.path.join(ROOT, "_build", "test", "libdevmath.so")
 
 @pytest.fixture(scope="module")
 def devmath():
-    hdrs = [os.path.join(ROOT, "grrt_b200", "csrc", "device", f) for f in ("kerr.cuh", "integrate.cuh", "mixed_spec.cuh", "scene.h")]
+    hdrs = [os.path.join(ROOT, "grrt_b200", "csrc", "device", f) for f in ("kerr.cuh", "integrate.cuh", "mixed_spec.cuh", "scene.h", "surrogate_geom.cuh")]
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(p) for p in hdrs + [SRC]):
         os.makedirs(os.path.dirname(OUT), exist_ok=True)
         subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O2", "-shared", "-Xcompiler", "-fPIC",

@@ -1,0 +1,68 @@
+"""The surrogate's closed-form ray classification
+(grrt_b200/csrc/device/surrogate_geom.cuh), compiled as host code, against
+the FP64 method's traces of the same camera rays. CPU only.
+
+A camera ray falls in iff the radial potential R(r) stays positive between the
+horizon and the camera; the minimum of R / (E^2 r^4) is the distance to the
+critical curve. Bars: the closed-form fate equals the integrated one (any
+disagreement lies within 0.01 of the curve and is rare), and every ray with
+three or more equatorial crossings outside 0.9 r_in that does not graze the
+plane lies inside the default critical band (|margin| < 0.15), so the network
+never has to model one.
+"""
+import ctypes as C
+import math
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+from oracle_bind import Oracle, jittered_samples
+from test_device_math import devmath  # noqa: F401  (fixture)
+
+CASES = [
+    ("kerr 0.998 80deg", dict(spin=0.998)),
+    ("schwarzschild 80deg", dict(metric_type=0, spin=0.0)),
+    ("kerr 0.9 67deg", dict(spin=0.9, observer_theta=math.radians(67.3))),
+    ("kerr 0.998 33deg", dict(spin=0.998, observer_theta=math.radians(33.3))),
+    ("kerr 0.5 edge-on", dict(spin=0.5, observer_theta=math.pi / 2)),
+]
+CRITICAL_BAND = 0.15  # surr::RenderBands::capture
+GRAZE_BAND = 0.02
+
+
+@pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
+def test_closed_form_margins(grrt, devmath, name, kw):  # noqa: F811
+    n = 64
+    R = grrt.Renderer(grrt.config_params(2, width=n, height=n, spp=1, background_type=0, **kw))
+    M, a, rh, _isco, robs, tol, max_steps = R.table("scalars")[:7]
+    r_in = R.table("flux_meta")[1]
+    sc = np.array([M, a, rh + 0.01, 1000.0, 0.01 * robs, tol, max_steps, 0.9 * r_in])
+    PD = C.POINTER(C.c_double)
+    devmath.devmath_ray_margins.argtypes = [C.c_double, C.c_double, C.c_double, PD, PD]
+    devmath.devmath_trace_crossings.argtypes = [PD, PD, PD]
+    px, py = jittered_samples(n, n, 1, np.arange(n * n))
+    O = Oracle(R)
+
+    def one(k):
+        y8 = O.camera_ray(px[k], py[k])
+        m, o = np.zeros(2), np.zeros(5)
+        devmath.devmath_ray_margins(M, a, rh, y8.ctypes.data_as(PD), m.ctypes.data_as(PD))
+        devmath.devmath_trace_crossings(sc.ctypes.data_as(PD), y8.ctypes.data_as(PD), o.ctypes.data_as(PD))
+        return np.concatenate([m, o])
+
+    with ThreadPoolExecutor(8) as ex:
+        res = np.array(list(ex.map(one, range(n * n), chunksize=64)))
+    cap, graze, term, nc = res[:, 0], res[:, 1], res[:, 2].astype(int), res[:, 3]
+    # the host trace is the oracle's method: its fates are the oracle's
+    _, oterm, _, _, _ = O.trace_rgb(px, py)
+    assert np.mean(oterm == term) > 0.998
+    ok = term != 2
+    bad = ok & ((cap > 0) != (term == 0))
+    multi = (nc >= 3) & (graze >= GRAZE_BAND)
+    worst_bad = float(np.max(np.abs(cap[bad]))) if bad.any() else 0.0
+    worst_multi = float(np.max(np.abs(cap[multi]))) if multi.any() else 0.0
+    print(f"\n  [{name}] captured {np.mean(term == 0):.3f}; fate disagreements {int(bad.sum())} (|m| <= {worst_bad:.2e}); "
+          f"3+ crossings {int(multi.sum())} (|m| <= {worst_multi:.3f}); in critical band {np.mean(np.abs(cap) < CRITICAL_BAND):.4f}")
+    assert worst_bad < 0.01 and bad.mean() < 0.005
+    assert worst_multi < CRITICAL_BAND
