@@ -63,12 +63,14 @@ __device__ void ray_margins(const DevScene& S, const double p[4], float& cap, fl
 }
 
 // Targets of a finished trace (network space).
-__device__ void finish_targets(const DevScene& S, int term, int nc, double r1, double r2, const Vec5<double>& y,
-                               double pt, double pph, float* Yq) {
+__device__ void finish_targets(const DevScene& S, int term, int nc, int n_extra, double r1, double r2,
+                               const Vec5<double>& y, double pt, double pph, float* Yq) {
+    // u = M / r, saturated at the relevance cut: a crossing that moves into the
+    // hole and one that never happens before capture give the same u_cut
     const double u_cut = S.M / (kRelevant * S.r_in);
     const double none = (term == kTermEscaped) ? 0.0 : u_cut;
-    Yq[kOutU1] = static_cast<float>(nc >= 1 ? S.M / r1 : none);
-    Yq[kOutU2] = static_cast<float>(nc >= 2 ? S.M / r2 : none);
+    Yq[kOutU1] = static_cast<float>(nc >= 1 ? fmin(S.M / r1, u_cut) : none);
+    Yq[kOutU2] = static_cast<float>(nc >= 2 ? fmin(S.M / r2, u_cut) : none);
     if (term == kTermEscaped) {
         const Vec5<double> d = kerr_rhs<double>(S.M, S.a, pt, pph, y);
         const Vec5<float> k{static_cast<float>(d.r), static_cast<float>(d.th), static_cast<float>(d.ph),
@@ -87,15 +89,15 @@ __device__ void finish_targets(const DevScene& S, int term, int nc, double r1, d
         Yq[kOutCosTh] = Yq[kOutSinPh] = Yq[kOutCosPh] = Yq[kOutCTh] = 0.0f;
     }
     Yq[6] = static_cast<float>(term);
-    Yq[7] = static_cast<float>(nc);
+    Yq[7] = static_cast<float>(n_extra);
 }
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // training data: the plain FP64 method (as the thin-disk kernel) recording the
-// first two equatorial crossings outside kRelevant * r_in and the escape
-// direction
+// first two equatorial crossings, the number of later ones outside
+// kRelevant * r_in, and the escape direction
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTraceThreads, 4)
 surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, int jitter_s, float* __restrict__ X,
@@ -108,7 +110,7 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
     const DevScene* S = scenes;
     Vec5<double> y;
     double pt = 0, pph = 0, dl = 0, r1 = 0, r2 = 0;
-    int retry = 0, step = 0, nc = 0;
+    int retry = 0, step = 0, nc = 0, n_extra = 0;
     while (true) {
         const bool want = !live && !exhausted;
         const unsigned nq = fetch_work(want, queue, total);
@@ -138,6 +140,7 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
                 retry = 0;
                 step = 0;
                 nc = 0;
+                n_extra = 0;
                 r1 = r2 = 0.0;
                 live = true;
             }
@@ -158,14 +161,14 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
                 ++n_acc;
                 const double d_prev = y.th - kHalfPi, d_new = y5.th - kHalfPi;
                 if (d_prev * d_new < 0.0 && fabs(d_prev - d_new) > 1e-12) {
+                    // crossings in time order at any radius (a crossing that goes
+                    // to infinity or into the hole leaves its slot continuously);
+                    // later ones only matter where a disk can emit
                     const double rc = y.r + (-d_prev / (d_new - d_prev)) * (y5.r - y.r);
-                    // only crossings that can reach the disk count (inside kRelevant
-                    // r_in no disk emits; a falling ray's late crossings lie there)
-                    if (rc >= kRelevant * S->r_in) {
-                        if (nc == 0) r1 = rc;
-                        else if (nc == 1) r2 = rc;
-                        ++nc;
-                    }
+                    if (nc == 0) r1 = rc;
+                    else if (nc == 1) r2 = rc;
+                    else if (rc >= kRelevant * S->r_in) ++n_extra;
+                    ++nc;
                 }
                 y = y5;
                 dl = d.next;
@@ -178,7 +181,7 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
         }
         if (live && term >= 0) {
             live = false;
-            finish_targets(*S, term, nc, r1, r2, y, pt, pph, Y + kYCols * static_cast<size_t>(q));
+            finish_targets(*S, term, nc, n_extra, r1, r2, y, pt, pph, Y + kYCols * static_cast<size_t>(q));
         }
     }
 #pragma unroll
@@ -263,20 +266,31 @@ __global__ void loss_kernel(const float* __restrict__ O, const float* __restrict
         const int term = static_cast<int>(y[6]);
         // rays near the critical curve, grazing the plane, or with three or more
         // crossings are re-traced exactly at render time: not fitted
-        const bool fit = fabsf(y[8]) >= kFitCapture && y[9] >= kFitGraze && y[7] < 3.0f;
+        const bool fit = fabsf(y[8]) >= kFitCapture && y[9] >= kFitGraze && y[7] == 0.0f;
         const bool u_ok = fit && (term == kTermHorizon || term == kTermEscaped);
         const bool esc = fit && term == kTermEscaped;
         const float inv = 1.0f / rows;
         __nv_bfloat16* g = dO + static_cast<size_t>(r) * kDOutPad;
 #pragma unroll
         for (int j = 0; j < kOutPad; ++j) {
-            float wt = 0.0f;
-            if (j < 2) wt = u_ok ? w.u : 0.0f;
-            else if (j < 5) wt = esc ? w.dir : 0.0f;
-            else if (j == 5) wt = esc ? w.cth : 0.0f;
-            const float d = (j < kUsedOut) ? o[j] - y[j] : 0.0f;
-            l += wt * d * d;
-            g[j] = __float2bfloat16_rn(2.0f * wt * d * inv);
+            float gj = 0.0f;
+            if (j < kTargets) {
+                float wt = 0.0f;
+                if (j < 2) wt = u_ok ? w.u : 0.0f;
+                else if (j < 5) wt = esc ? w.dir : 0.0f;
+                else wt = esc ? w.cth : 0.0f;
+                const float d = o[j] - y[j];
+                l += wt * d * d;
+                gj = 2.0f * wt * d * inv;
+            } else if (j < kUsedOut && u_ok) {
+                // log-sigma head of u slot j - kTargets: NLL with the residual fixed
+                const float d = o[j - kTargets] - y[j - kTargets];
+                const float s = fminf(fmaxf(o[j], -12.0f), 4.0f);
+                const float e = __expf(-2.0f * s);
+                l += w.sig * 0.5f * (d * d * e + 2.0f * s);
+                gj = w.sig * (1.0f - d * d * e) * inv;
+            }
+            g[j] = __float2bfloat16_rn(gj);
         }
         l *= inv;
     }
@@ -538,11 +552,13 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
             if (!(o[0] == o[0]) || !(o[1] == o[1])) exact = true;  // NaN
             for (int c = 0; c < 2 && !exact; ++c) {
                 const double u = o[c];
-                if (!(u > 1e-6)) continue;  // no crossing: escapes first
-                const double r = S.M / u;
-                // radius band from the calibrated u error: r in [M/(u+du), M/(u-du)]
-                const double r_lo = S.M / (u + bands.du);
-                const double r_hi = (u > bands.du) ? S.M / (u - bands.du) : 1e30;
+                // this sample's u error band: the calibrated multiple of its predicted sigma
+                const double du = bands.du * exp(fmin(fmax(static_cast<double>(o[kOutLogSig1 + c]), -12.0), 4.0));
+                if (!(u + du > 0.0)) continue;  // no crossing: escapes first
+                const double r = S.M / fmax(u, 1e-12);
+                // radius band: r in [M/(u+du), M/(u-du)]
+                const double r_lo = S.M / (u + du);
+                const double r_hi = (u > du) ? S.M / (u - du) : 1e30;
                 if (r_hi < S.r_in || r_lo > S.r_out) continue;  // surely outside the disk
                 if (r_lo <= S.r_in || r_hi >= S.r_out) {  // may cross an edge
                     exact = true;
@@ -614,8 +630,8 @@ __global__ void eval_errors_kernel(const float* __restrict__ O, const float* __r
     const int term = static_cast<int>(y[6]);
     float* e = err + q * 4;
     const bool u_ok = term == kTermHorizon || term == kTermEscaped;
-    e[0] = u_ok ? fabsf(o[0] - y[0]) : -1.0f;
-    e[1] = u_ok ? fabsf(o[1] - y[1]) : -1.0f;
+    e[0] = u_ok ? fabsf(o[0] - y[0]) * __expf(-fminf(fmaxf(o[kOutLogSig1], -12.0f), 4.0f)) : -1.0f;
+    e[1] = u_ok ? fabsf(o[1] - y[1]) * __expf(-fminf(fmaxf(o[kOutLogSig2], -12.0f), 4.0f)) : -1.0f;
     if (term == kTermEscaped) {
         // angle between the predicted and true arc-start directions
         const float st_p = sqrtf(fmaxf(0.0f, 1.0f - o[2] * o[2])), st_t = sqrtf(fmaxf(0.0f, 1.0f - y[2] * y[2]));

@@ -17,13 +17,15 @@ namespace surr {
 
 constexpr int kIn = 4;
 constexpr int kHidden = 256;
-constexpr int kUsedOut = 6;   // network outputs (u1, u2, cos theta, sin phi, cos phi, c_theta)
+constexpr int kTargets = 6;   // fitted quantities (u1, u2, cos theta, sin phi, cos phi, c_theta)
+constexpr int kUsedOut = 8;   // outputs: the targets, then log sigma of the u1 and u2 errors
 constexpr int kOutPad = 16;   // output layer rows computed by the GEMM (kUsedOut used)
 constexpr int kDOutPad = 64;  // K of the output layer's backward GEMM
-constexpr int kYCols = 10;    // 6 targets, termination, crossings, capture margin, graze margin
-// Crossings inside kRelevant * r_in are not recorded (no disk emits there):
-// targets u1, u2 are the first two crossings outside it, u = M/(kRelevant r_in)
-// when a captured ray has none.
+constexpr int kYCols = 10;    // 6 targets, termination, later crossings, capture margin, graze margin
+// Targets u1, u2: u = M / r of the first and second equatorial crossing in
+// time order, saturated at M / (kRelevant r_in) (no disk emits inside); 0 when
+// the ray escapes first, the saturation value when it falls in first. Later
+// crossings count only outside kRelevant * r_in (record column 7).
 constexpr double kRelevant = 0.9;
 
 // Offsets (floats) of the parameters in one FP32 array.
@@ -42,20 +44,23 @@ struct ParamLayout {
     }
 };
 
-// Loss weights of the six outputs.
+// Loss weights: squared error of the six targets, and the Gaussian negative
+// log-likelihood 0.5 (d^2 exp(-2 s) + 2 s) of the two log-sigma heads, with
+// the u residual d held fixed (the heads learn the error, not the value).
 struct LossWeights {
-    float u = 16.0f, dir = 0.5f, cth = 0.25f;
+    float u = 16.0f, dir = 0.5f, cth = 0.25f, sig = 0.1f;
 };
 // Samples fitted: capture margin |m| >= kFitCapture, graze margin >=
-// kFitGraze, fewer than three crossings (the rest is the exact path's; the
-// calibrated bands never fall below these).
+// kFitGraze, no relevant crossing after the second (the rest is the exact
+// path's; the calibrated bands never fall below these).
 constexpr float kFitCapture = 0.05f;
 constexpr float kFitGraze = 0.02f;
 
 // Data: every sample of n_cams cameras x (n_side x n_side) pixels, jittered by
 // the reference's pixel hash with sample index `jitter_s` (0 train, 1 validation).
 // X[q][4] network inputs; Y[q][10] the six targets, termination, number of
-// equatorial crossings outside kRelevant * r_in, capture margin, graze margin.
+// crossings after the second outside kRelevant * r_in, capture margin, graze
+// margin.
 cudaError_t launch_trace_dataset(const DevScene* d_scenes, int n_cams, int n_side, int jitter_s, float* X, float* Y,
                                  unsigned* queue, DevStats* stats, cudaStream_t s);
 
@@ -86,7 +91,7 @@ cudaError_t launch_cast_weights(const float* params, __nv_bfloat16* const* wb, _
 // closed-form margins; then, from the network outputs, the colour or a
 // place in the exact re-trace queue.
 struct RenderBands {
-    double du = 1e-3;          // calibrated |u error| (u = M / r)
+    double du = 4.0;           // u error band = du * sigma (the sample's predicted error)
     double dir = 1e-3;         // calibrated escape-direction error (rad)
     double capture = 0.15;     // |capture margin| below this: exact
     double graze = 0.02;       // graze margin below this: exact
@@ -103,8 +108,8 @@ cudaError_t launch_shade(const DevScene& S, const DevTile& tile, size_t q0, size
                          cudaStream_t s);
 
 // Validation: per sample, errors of the network outputs against the targets
-// (err[q][0] = |du1|, [1] = |du2|, [2] = arc-start direction error (rad),
-// [3] = |c_theta error|; -1 where the target does not apply).
+// (err[q][0] = |du1| / sigma1, [1] = |du2| / sigma2, [2] = arc-start direction
+// error (rad), [3] = |c_theta error|; -1 where the target does not apply).
 cudaError_t launch_eval_errors(const float* O, const float* Y, size_t n, float* err, cudaStream_t s);
 
 }  // namespace surr

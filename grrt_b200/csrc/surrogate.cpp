@@ -571,11 +571,12 @@ struct GRRTSurrogate {
         dfree(Y);
         if (!ok) return false;
         // 1. critical band: holds every sample whose closed-form fate disagrees
-        //    with the integrator's (x2) and every sample with three or more
-        //    relevant crossings that does not graze (x1.2); never below the
+        //    with the integrator's (x2) and every sample with a relevant crossing
+        //    after the second that does not graze (x1.2); never below the
         //    training fit cut
         // 2. graze band: the training fit cut (mu of the turning point)
-        // 3. network error quantiles over the samples outside both bands
+        // 3. network error quantiles over the samples outside both bands (u:
+        //    the error in units of the network's own predicted sigma)
         float cap_bad = 0.0f, multi = 0.0f;
         size_t n_cap_bad = 0, n_multi = 0;
         for (size_t i = 0; i < n; ++i) {
@@ -586,7 +587,7 @@ struct GRRTSurrogate {
                 cap_bad = std::max(cap_bad, std::fabs(y[8]));
                 ++n_cap_bad;
             }
-            if (y[7] >= 3.0f && y[9] >= kFitGraze) {
+            if (y[7] >= 1.0f && y[9] >= kFitGraze) {
                 multi = std::max(multi, std::fabs(y[8]));
                 ++n_multi;
             }
@@ -608,7 +609,7 @@ struct GRRTSurrogate {
             }
         }
         const double median_du = quantile(du, 0.5);
-        bands.du = safety * quantile(du, q);
+        bands.du = safety * quantile(du, q);  // multiple of the predicted sigma
         const double du_arc = 1.0 / 1000.0 - 1.0 / 7000.0;
         bands.dir = safety * (quantile(dir, q) + quantile(cth, q) * du_arc);
         bands.capture = cap_band;

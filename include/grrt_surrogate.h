@@ -35,12 +35,15 @@ GRRT_EXPORT int grrt_surrogate_gemm_bf16(const void* A, int lda, const void* B, 
  * Network: inputs (alpha, beta) (image-plane angles, radians, both scaled by
  * the width as in the reference camera), spin, inclination, each mapped to
  * [-1, 1]; hidden 4 x 256 SiLU; outputs
- *   0, 1: u = M / r of the first and second equatorial crossing outside
- *         0.9 r_in (0 when the ray escapes first, M / (0.9 r_in) when it falls
- *         in first; inside 0.9 r_in no disk emits)
+ *   0, 1: u = M / r of the first and second equatorial crossing in time
+ *         order, saturated at M / (0.9 r_in) (no disk emits inside); 0 when
+ *         the ray escapes first, the saturation value when it falls in first
  *   2-4:  cos(theta), sin(phi), cos(phi) of the sky position at r = 1000 M
  *         (folded as the star lookup folds it)
- *   5:    c_theta / 32 with c_theta = r^2 dtheta/dr there (far-field bending).
+ *   5:    c_theta / 32 with c_theta = r^2 dtheta/dr there (far-field bending)
+ *   6, 7: log sigma of the network's own error on outputs 0 and 1, trained by
+ *         a Gaussian likelihood on the residual; a sample's u band is a
+ *         calibrated multiple of its sigma.
  * The redshift factor g is not learned: at a crossing radius it follows in
  * closed form from the ray's constants (p_t, p_phi), as in the plain form. */
 typedef struct GRRTSurrogate GRRTSurrogate;
@@ -57,7 +60,8 @@ GRRT_EXPORT const char* grrt_surrogate_error(const GRRTSurrogate* s);
 GRRT_EXPORT int grrt_surrogate_generate(GRRTSurrogate* s, const GRRTParams* cams, int n_cams, int n_side);
 /* Number of samples in the training set; with buffers of `capacity` samples,
  * copies inputs (float[4] each) and records (float[10] each: the six targets,
- * termination, crossings outside 0.9 r_in, capture margin, graze margin). */
+ * termination, crossings after the second outside 0.9 r_in, capture margin,
+ * graze margin). */
 GRRT_EXPORT long long grrt_surrogate_dataset(GRRTSurrogate* s, float* x_out, float* y_out, long long capacity);
 
 /* `steps` Adam steps (beta 0.9 / 0.999) on random batches of `batch` samples
@@ -69,21 +73,25 @@ GRRT_EXPORT int grrt_surrogate_train(GRRTSurrogate* s, int steps, int batch, dou
 /* Calibrates the fallback bands on a fresh validation set of the given
  * cameras (jitter sample 1). Critical band: covers every sample whose
  * closed-form fate disagrees with the integrator's (x2) and every sample with
- * three or more relevant crossings that does not graze (x1.2), at least 0.05.
- * Graze band: turning point within mu = 0.02 of the equator. u and direction
- * errors: the `quantile` of the samples outside both bands, times `safety`.
- * report8 (or NULL): du, dir, capture band, graze band, validation samples,
- * fate disagreements, fraction of samples in the bands, median u error
- * outside them. */
+ * a crossing outside 0.9 r_in after the second that does not graze (x1.2), at
+ * least 0.05.
+ * Graze band: turning point within mu = 0.02 of the equator. u band: the
+ * `quantile` of |u error| / sigma over the samples outside both bands, times
+ * `safety` (a multiple of each sample's predicted sigma); direction band: the
+ * `quantile` of the direction error times `safety`. report8 (or NULL): u band
+ * multiple, direction band, capture band, graze band, validation samples,
+ * fate disagreements, fraction of samples in the bands, median |u error| /
+ * sigma outside them. */
 GRRT_EXPORT int grrt_surrogate_calibrate(GRRTSurrogate* s, const GRRTParams* cams, int n_cams, int n_side,
                                          double quantile, double safety, double* report8);
 GRRT_EXPORT int grrt_surrogate_set_bands(GRRTSurrogate* s, double du, double dir, double capture, double graze,
                                          double tol_rel);
-/* out5: du, dir, capture, graze, tol_rel. Returns 1 if calibrated or set, 0 if default. */
+/* out5: du (multiple of sigma), dir, capture, graze, tol_rel. Returns 1 if
+ * calibrated or set, 0 if default. */
 GRRT_EXPORT int grrt_surrogate_get_bands(const GRRTSurrogate* s, double* out5);
 
 /* FP32 parameters: W1[256x4], b1, W2..W4[256x256], b2..b4, W5[16x256]
- * (rows 6..15 zero), b5[16]. Returns the count; copies when capacity allows. */
+ * (rows 8..15 zero), b5[16]. Returns the count; copies when capacity allows. */
 GRRT_EXPORT long long grrt_surrogate_params(GRRTSurrogate* s, float* out, long long capacity);
 GRRT_EXPORT int grrt_surrogate_set_params(GRRTSurrogate* s, const float* in, long long n);
 /* Network outputs float[n][16] for device inputs float[n][4] (the fused

@@ -13,8 +13,9 @@ import numpy as np
 
 HID = 256
 OUT_PAD = 16
-USED = 6
-WEIGHTS = {"u": 16.0, "dir": 0.5, "cth": 0.25}  # surr::LossWeights
+USED = 6      # fitted targets
+HEADS = 8     # outputs used: targets + log-sigma heads of u1, u2
+WEIGHTS = {"u": 16.0, "dir": 0.5, "cth": 0.25, "sig": 0.1}  # surr::LossWeights
 FIT_CAPTURE, FIT_GRAZE = 0.05, 0.02  # surr::kFitCapture, kFitGraze
 
 
@@ -73,7 +74,7 @@ def row_weights(Y):
     Y = np.asarray(Y, dtype=np.float64)
     term = Y[:, 6].astype(int)
     w = np.zeros((len(Y), OUT_PAD))
-    fit = (np.abs(Y[:, 8]) >= FIT_CAPTURE) & (Y[:, 9] >= FIT_GRAZE) & (Y[:, 7] < 3)
+    fit = (np.abs(Y[:, 8]) >= FIT_CAPTURE) & (Y[:, 9] >= FIT_GRAZE) & (Y[:, 7] == 0)
     u_ok = fit & ((term == 0) | (term == 1))
     esc = fit & (term == 1)
     w[:, 0] = w[:, 1] = np.where(u_ok, WEIGHTS["u"], 0.0)
@@ -82,18 +83,33 @@ def row_weights(Y):
     return w
 
 
+def loss_terms(o, Y):
+    """Loss and d(loss)/d(output) (the log-sigma heads get the likelihood
+    gradient with the u residual held fixed, as the GPU loss kernel)."""
+    B = len(o)
+    w = row_weights(Y)
+    d = np.zeros_like(o)
+    d[:, :USED] = o[:, :USED] - Y[:, :USED]
+    loss = np.sum(w * d * d)
+    g = 2.0 * w * d
+    u_ok = w[:, 0] > 0
+    for j in (6, 7):
+        s = np.clip(o[:, j], -12.0, 4.0)
+        e = np.exp(-2.0 * s)
+        dj = d[:, j - 6]
+        loss += np.sum(np.where(u_ok, WEIGHTS["sig"] * 0.5 * (dj * dj * e + 2.0 * s), 0.0))
+        g[:, j] = np.where(u_ok, WEIGHTS["sig"] * (1.0 - dj * dj * e), 0.0)
+    return float(loss / B), g / B
+
+
 def loss_and_grads(p, X, Y, bf=True):
     P = unpack(p)
     r = bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
     X = np.asarray(X, dtype=np.float64)
     Y = np.asarray(Y, dtype=np.float64)
-    B = len(X)
     o, zs, hs = forward(p, X, bf)
-    w = row_weights(Y)
-    d = np.zeros_like(o)
-    d[:, :USED] = o[:, :USED] - Y[:, :USED]
-    loss = float(np.sum(w * d * d) / B)
-    dO = r(2.0 * w * d / B)
+    loss, g_o = loss_terms(o, Y)
+    dO = r(g_o)
     g = {}
     g["W5"] = dO.T @ hs[3]
     g["b5"] = dO.sum(0)
@@ -108,11 +124,12 @@ def loss_and_grads(p, X, Y, bf=True):
 
 
 def loss_only(p, X, Y):
+    """The loss as a function of the parameters. The log-sigma heads see the u
+    residual as a constant, so finite differences of this function match the
+    training gradient only for the parameters the heads alone use (their rows
+    of W5 and b5) or with the head weight set to zero."""
     o, _, _ = forward(p, X, bf=False)
-    w = row_weights(Y)
-    d = np.zeros_like(o)
-    d[:, :USED] = o[:, :USED] - np.asarray(Y, dtype=np.float64)[:, :USED]
-    return float(np.sum(w * d * d) / len(X))
+    return loss_terms(o, np.asarray(Y, dtype=np.float64))[0]
 
 
 def random_params(seed, scale=1.0):
@@ -122,9 +139,9 @@ def random_params(seed, scale=1.0):
         d[f"W{l}"] = rng.uniform(-1, 1, (HID, HID)) * np.sqrt(3 / HID) * scale
         d[f"b{l}"] = rng.normal(0, 0.1, HID)
     W5 = np.zeros((OUT_PAD, HID))
-    W5[:USED] = rng.uniform(-1, 1, (USED, HID)) * np.sqrt(3 / HID) * scale
+    W5[:HEADS] = rng.uniform(-1, 1, (HEADS, HID)) * np.sqrt(3 / HID) * scale
     b5 = np.zeros(OUT_PAD)
-    b5[:USED] = rng.normal(0, 0.1, USED)
+    b5[:HEADS] = rng.normal(0, 0.1, HEADS)
     d["W5"], d["b5"] = W5, b5
     return pack(d)
 
@@ -135,7 +152,7 @@ def random_batch(seed, n):
     Y = np.zeros((n, 10))
     Y[:, :USED] = rng.normal(0, 0.5, (n, USED))
     Y[:, 6] = rng.choice([0, 1, 1, 1, 2], n)  # mostly escapes, some captures, a few masked
-    Y[:, 7] = rng.choice([0, 1, 2, 3], n, p=[0.3, 0.4, 0.25, 0.05])
+    Y[:, 7] = rng.choice([0, 1], n, p=[0.95, 0.05])  # relevant crossings after the second
     Y[:, 8] = rng.uniform(-1, 1, n)  # capture margin (a few inside the fit cut)
     Y[:, 9] = rng.uniform(0, 1, n)   # graze margin
     return X, Y

@@ -92,16 +92,16 @@ void devmath_ray_margins(double M, double a, double r_h, const double* y8, doubl
 }
 
 // The surrogate's training trace (the FP64 method, as the thin-disk kernel)
-// of one camera ray: sc = (M, a, r_stop, r_escape, dl0, tol, max_steps, r_cut)
-// with r_cut the smallest crossing radius recorded. out = (termination,
-// crossings outside r_cut, first and second such radius, accepted steps).
+// of one camera ray: sc = (M, a, r_stop, r_escape, dl0, tol, max_steps, r_cut).
+// out = (termination, crossings outside r_cut, first and second such radius,
+// accepted steps, crossings after the second in time order outside r_cut).
 void devmath_trace_crossings(const double* sc, const double* y8, double* out) {
     const double M = sc[0], a = sc[1], r_stop = sc[2], r_esc = sc[3], dl0 = sc[4], tol = sc[5], r_cut = sc[7];
     const int max_steps = static_cast<int>(sc[6]);
     const double pt = y8[4], pph = y8[7];
     Vec5<double> y{y8[1], y8[2], y8[3], y8[5], y8[6]};
     double dl = dl0, r1 = 0.0, r2 = 0.0;
-    int retry = 0, step = 0, nc = 0, term = -1;
+    int retry = 0, step = 0, nc = 0, term = -1, n_all = 0, n_extra = 0;
     while (true) {
         if (retry == 0) {
             if (step >= max_steps) { term = kTermMaxSteps; break; }
@@ -115,6 +115,8 @@ void devmath_trace_crossings(const double* sc, const double* y8, double* out) {
             const double dp = y.th - 0.5 * mixed::kPi, dn = y5.th - 0.5 * mixed::kPi;
             if (dp * dn < 0.0 && fabs(dp - dn) > 1e-12) {
                 const double rc = y.r + (-dp / (dn - dp)) * (y5.r - y.r);
+                if (n_all >= 2 && rc >= r_cut) ++n_extra;
+                ++n_all;
                 if (rc >= r_cut) {
                     if (nc == 0) r1 = rc;
                     else if (nc == 1) r2 = rc;
@@ -135,5 +137,6 @@ void devmath_trace_crossings(const double* sc, const double* y8, double* out) {
     out[2] = r1;
     out[3] = r2;
     out[4] = step;
+    out[5] = n_extra;
 }
 }

@@ -6,7 +6,10 @@ import numpy as np
 import mlp_ref
 
 
-def test_restatement_gradients_match_finite_differences():
+def test_restatement_gradients_match_finite_differences(monkeypatch):
+    # with the head weight zero the loss is the plain masked squared error, a
+    # function of the parameters alone (the heads' gradient is checked below)
+    monkeypatch.setitem(mlp_ref.WEIGHTS, "sig", 0.0)
     p = mlp_ref.random_params(3)
     X, Y = mlp_ref.random_batch(4, 24)
     _, g = mlp_ref.loss_and_grads(p, X, Y, bf=False)
@@ -38,3 +41,21 @@ def test_bf16_rounding_is_round_to_nearest_even():
     assert got[3] == 1.0 + 2 ** -6  # tie -> even
     assert got[4] == -2.5
     assert abs(got[5] - 3.140625) < 1e-12
+
+
+def test_sigma_head_gradient_matches_finite_differences():
+    """The log-sigma heads (rows 6, 7 of W5 and b5) see the u residual as a
+    constant: their own parameters' gradients are finite differences of the loss."""
+    p = mlp_ref.random_params(11)
+    X, Y = mlp_ref.random_batch(12, 32)
+    _, g = mlp_ref.loss_and_grads(p, X, Y, bf=False)
+    w5 = 256 * 4 + 256 + 3 * (65536 + 256)
+    b5 = w5 + 16 * 256
+    idx = [w5 + 6 * 256 + k for k in (0, 17, 255)] + [w5 + 7 * 256 + k for k in (3, 100)] + [b5 + 6, b5 + 7]
+    for i in idx:
+        h = 1e-6
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (mlp_ref.loss_only(pp, X, Y) - mlp_ref.loss_only(pm, X, Y)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-5 * max(abs(fd), 1e-6), (i, fd, g[i])
