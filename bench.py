@@ -12,6 +12,11 @@ generated from its parameters; no dataset).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64]
   python bench.py --impl reference   # the reference's own CPU code, same workload
 
+The line also carries "surrogate": the learned form, trained in the same run
+on the 64-camera sweep and timed on its evaluation frame (Kerr a=0.998, 80
+deg, 2048^2, 1 spp, thin disk, black background) beside the FP64 and mixed
+forms of that frame (--surrogate-steps 0 skips it).
+
 `value` is rays/s of the headline form (default: mixed, whose output is held
 to <=1e-4 relative of the FP64 form and reported against it) with the scene
 and the output resident on the device (CUDA events around each render launch
@@ -70,6 +75,9 @@ def parse():
     ap.add_argument("--height", type=int, default=1024)
     # the batched sweep (64 cameras, one persistent launch) instead of the headline frame
     ap.add_argument("--batch", action="store_true")
+    # the learned surrogate (trained in this run) on its evaluation frame; 0 skips it
+    ap.add_argument("--surrogate-steps", type=int, default=8000)
+    ap.add_argument("--surrogate-size", type=int, default=2048)
     return ap.parse_args()
 
 
@@ -353,6 +361,109 @@ def sgemm_peak(torch) -> float:
     return best
 
 
+# One forward pass of the surrogate MLP per sample, algorithmic FLOPs:
+# 2 x (4 x 256 + 3 x 256 x 256 + 256 x 8) multiply-adds (8 outputs used).
+F_MLP = 2 * (4 * 256 + 3 * 256 * 256 + 256 * 8)
+
+
+def run_surrogate(args, torch, G, stream, flush, peaks):
+    """Learned surrogate: trained here on the 64-camera sweep (4 spins x 16
+    inclinations, 512^2 samples each, black background) by the library's own
+    kernels, calibrated on the same cameras at 256^2 (other jitter), then
+    timed on its evaluation frame (Kerr a=0.998, 80 deg, thin disk, 1 spp,
+    black background) against the FP64 and mixed forms of the same frame."""
+    n = args.surrogate_size
+    cams = [dict(c, background_type=0) for c in G.sweep_cameras(width=512, height=512)]
+    S = G.Surrogate(11)
+    t = time.perf_counter()
+    S.generate(cams, 512)
+    t_gen = time.perf_counter() - t
+    t = time.perf_counter()
+    hist = S.train(args.surrogate_steps, batch=16384, lr=1e-3)
+    t_train = time.perf_counter() - t
+    cal = S.calibrate(cams, 256)
+    frame = G.config_params(2, width=n, height=n, spp=1, background_type=0)
+    R = G.Renderer(frame)
+    ref = torch.empty((n, n, 3), dtype=torch.float64, device="cuda")
+    rfate = torch.empty((n * n,), dtype=torch.int32, device="cuda")
+    out = torch.empty_like(ref)
+    ofate = torch.empty_like(rfate)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.mean(ts))
+
+    R.set_precision(G.FORM_FP64)
+    ms_fp64 = timed(lambda: R.render_device(None, ref, rfate, stream))
+    st64 = R.stats()
+    R.set_precision(G.FORM_MIXED)
+    mix = torch.empty_like(ref)
+    ms_mixed = timed(lambda: R.render_device(None, mix, None, stream))
+    ms_surr = timed(lambda: S.render_device(R, None, out, ofate, stream))
+    phases = R.phase_ms()
+    st = R.stats()
+    exact, samples = S.last_exact()
+    # network alone on the frame's sample count (CUDA events around the fused kernel)
+    xin = torch.rand((n * n, 4), device="cuda") * 2 - 1
+    xo = torch.empty((n * n, 16), device="cuda")
+    S.forward(xin, xo, n * n)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    S.forward(xin, xo, n * n)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_mlp = e0.elapsed_time(e1)
+    a, b = out.cpu().numpy(), ref.cpu().numpy()
+    scale = float(b.max())
+    rel = (np.abs(a - b) / np.maximum(np.abs(b), 1e-6 * scale)).max(axis=2)
+    lit = b.max(axis=2) > 1e-6 * scale
+    mlp_tflops = F_MLP * n * n / (ms_mlp * 1e-3) / 1e12
+    peak = peaks.get("bf16_tflops")
+    rays = n * n
+    return {
+        "config": {"workload": f"kerr_a0.998_80deg_{n}x{n}_1spp_thin_disk_isco_20M_black_background",
+                   "rays_per_step": rays, "training": "64 cameras (spins 0, 0.5, 0.9, 0.998 x 16 inclinations "
+                   "5..90 deg) x 512^2 samples traced by the FP64 form", "train_steps": args.surrogate_steps,
+                   "batch": 16384, "l2": "flushed between steps (256 MiB write)"},
+        "value": rays / (ms_surr * 1e-3), "unit": "rays/s", "ms_per_step": ms_surr,
+        "fp64": {"value": rays / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64},
+        "mixed": {"value": rays / (ms_mixed * 1e-3), "ms_per_step": ms_mixed},
+        "speedup_vs_fp64": ms_fp64 / ms_surr, "speedup_vs_mixed": ms_mixed / ms_surr,
+        "phase_ms": {"network_and_shading": phases[0], "exact_retrace": phases[2], "resolve": phases[3]},
+        "exact_fraction": exact / max(1, samples),
+        "attempts": {"surrogate": st["attempts"], "fp64": st64["attempts"]},
+        "error_vs_fp64": {"max_rel": float(rel.max()), "pixels_over_1e-3": int((rel > 1e-3).sum()),
+                          "lit_pixels": int(lit.sum()),
+                          "lit_rel_quantiles_50_99_100": [float(x) for x in np.quantile(rel[lit], [0.5, 0.99, 1.0])],
+                          "sample_fates_differing": int((ofate != rfate).sum().item()),
+                          "rel_floor": "max(|fp64|, 1e-6 x frame max)"},
+        "calibration": cal,
+        "train": {"seconds": t_train, "generate_seconds": t_gen, "loss_first": float(np.mean(hist[:20])),
+                  "loss_last": float(np.mean(hist[-20:])),
+                  "samples_per_s": args.surrogate_steps * 16384 / t_train,
+                  "tflops": 3 * F_MLP * 16384 * args.surrogate_steps / t_train / 1e12},
+        "mlp_roofline": {"kernel": "mlp_fused_kernel", "bound": "tensor", "achieved": mlp_tflops,
+                         "peak": peak, "unit": "TFLOP/s", "frac": (mlp_tflops / peak) if peak else None,
+                         "launch_ms": ms_mlp, "flops_per_launch": F_MLP * rays,
+                         "flop_count": f"{F_MLP} per sample (4x256 + 3x256x256 + 256x8 multiply-adds, x2) x {rays}",
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)"},
+        "gpu_launches_per_step": 6,
+    }
+
+
 def main():
     global W, H, RAYS, WORKLOAD
     args = parse()
@@ -492,6 +603,11 @@ def main():
                          "crossings": head["stats"]["crossings"],
                          "fp64_attempt_share": head["stats"]["fp64_attempts"] / max(1, head["stats"]["attempts"])},
                 "kernel_ms_per_step": head["kernel_ms"], "wall_s_timed_region": head["wall"]}
+        if args.surrogate_steps > 0:
+            try:
+                line["surrogate"] = run_surrogate(args, torch, G, stream, flush, peaks)
+            except Exception as ex:  # reported, the headline stands on its own
+                line["surrogate"] = {"error": str(ex)}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
