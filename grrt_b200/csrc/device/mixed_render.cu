@@ -100,7 +100,7 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 __global__ void __launch_bounds__(kMixThreads, 4)
 mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb, DevStats* stats) {
     const int g2 = S.grid * S.grid;
-    const unsigned total = static_cast<unsigned>(tile.w) * tile.h * g2;
+    const unsigned total = mb.spec_list ? *mb.spec_count : static_cast<unsigned>(tile.w) * tile.h * g2;
     const float Mf = static_cast<float>(S.M), af = static_cast<float>(S.a);
     unsigned long long n_att = 0, n_acc = 0, n_rays = 0;
     unsigned q = ~0u;
@@ -116,7 +116,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, D
             if (nq == ~0u) {
                 exhausted = true;
             } else {
-                q = nq;
+                q = mb.spec_list ? mb.spec_list[nq] : nq;
                 sample_start(S, tile, q, g2, y, pt, pph);
                 dl = S.dl0;
                 retry = 0;
@@ -152,7 +152,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, D
         bool queue = false;
         if (live && term >= 0) {
             live = false;
-            ++n_rays;
+            if (!mb.spec_list) ++n_rays;  // a list's samples are counted by its producer
             const size_t o = 3 * static_cast<size_t>(q);
             if (retrace || term == kTermMaxSteps) {
                 queue = true;
@@ -340,7 +340,7 @@ __global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S, const D
 
 size_t mixed_scratch_bytes(const DevTile& tile, int g2) {
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
-    return n * (3 * sizeof(double) + 2 * sizeof(unsigned)) + 1024;
+    return n * (3 * sizeof(double) + 3 * sizeof(unsigned)) + 1024;
 }
 
 namespace {
@@ -372,6 +372,34 @@ DevMixedBuffers mixed_buffers(void* scratch, size_t n, unsigned* queue) {
     mb.sample_fate = reinterpret_cast<uint32_t*>(base + 1024 + n * 3 * sizeof(double));
     mb.retrace_list = mb.sample_fate + n;
     return mb;
+}
+
+DevMixedBuffers mixed_buffers_with_list(void* scratch, size_t n, unsigned* queue) {
+    DevMixedBuffers mb = mixed_buffers(scratch, n, queue);
+    mb.spec_count = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(scratch) + 768);
+    mb.spec_list = mb.retrace_list + n;
+    return mb;
+}
+
+cudaError_t launch_mixed_speculate(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                                   DevStats* stats, cudaStream_t stream) {
+    const MixLaunchShape& sh = mix_shape();
+    const size_t n = static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid;
+    const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
+    mixed_speculate_kernel<<<need < sh.sms * sh.per_spec ? need : sh.sms * sh.per_spec, kMixThreads, 0, stream>>>(
+        S, tile, mb, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_stars(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                               cudaStream_t stream) {
+    if (!S.stars_on) return cudaSuccess;
+    const MixLaunchShape& sh = mix_shape();
+    const size_t n = static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid;
+    int sb = static_cast<int>((n + 255) / 256);
+    if (sb > sh.sms * 8) sb = sh.sms * 8;
+    mixed_star_kernel<<<sb, 256, 0, stream>>>(S, tile, mb);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,

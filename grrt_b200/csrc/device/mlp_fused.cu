@@ -56,7 +56,7 @@ struct FusedMaps {
 };
 
 // the same SiLU as the training kernels
-__device__ __forceinline__ float silu_f(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_f(float z) { return sm100::silu_fast(z); }
 
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

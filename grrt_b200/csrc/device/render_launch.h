@@ -28,6 +28,10 @@ struct DevMixedBuffers {
     unsigned* queue2 = nullptr;         // phase-2 work counter
     unsigned* retrace_count = nullptr;  // samples queued for the FP64 re-trace
     unsigned* retrace_list = nullptr;   // their sample indices
+    // optional: the speculative pass traces spec_list[0 .. *spec_count) instead
+    // of every sample of the tile (the surrogate's uncertain samples)
+    unsigned* spec_list = nullptr;
+    unsigned* spec_count = nullptr;
     double* sample_rgb = nullptr;       // 3 per sample
     uint32_t* sample_fate = nullptr;    // per sample
     double margin = 0.05;               // disk-radius margin of the re-trace test
@@ -66,11 +70,21 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
                               double r_near, cudaEvent_t* phase_events, cudaStream_t stream);
 
 // The mixed form's buffers inside a scratch of mixed_scratch_bytes (queue is
-// the caller's phase-1 counter), and its re-trace and resolve phases on their
-// own: the re-trace traces retrace_list[0 .. *retrace_count) with the FP64
-// method into sample_rgb / sample_fate; the resolve sums samples into pixels.
-// queue2 and retrace_count (scratch bytes 256..1023) must be zeroed first.
+// the caller's phase-1 counter; spec_list left unset), and its re-trace and
+// resolve phases on their own: the re-trace traces
+// retrace_list[0 .. *retrace_count) with the FP64 method into sample_rgb /
+// sample_fate; the resolve sums samples into pixels. queue2, retrace_count and
+// the speculation-list counter (scratch bytes 256..1023) must be zeroed first.
 DevMixedBuffers mixed_buffers(void* scratch, size_t n_samples, unsigned* queue);
+// The same with a speculation list (after the re-trace list; its counter at
+// scratch byte 768).
+DevMixedBuffers mixed_buffers_with_list(void* scratch, size_t n_samples, unsigned* queue);
+// The speculative pass (over mb.spec_list when set; mb.queue zeroed first) and
+// the star pass on their own.
+cudaError_t launch_mixed_speculate(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                                   DevStats* stats, cudaStream_t stream);
+cudaError_t launch_mixed_stars(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                               cudaStream_t stream);
 cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
                                  cudaStream_t stream);
 cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,

@@ -138,5 +138,19 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n) {
            (static_cast<uint32_t>(m >> 4) << 24);
 }
 
+// SiLU through the hardware tanh (one special-function op):
+// silu(z) = z sigmoid(z), sigmoid(z) = (1 + tanh(z / 2)) / 2.
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigmoid_fast(float z) { return fmaf(0.5f, tanh_fast(0.5f * z), 0.5f); }
+__device__ __forceinline__ float silu_fast(float z) { return z * sigmoid_fast(z); }
+__device__ __forceinline__ float silu_grad_fast(float z) {
+    const float s = sigmoid_fast(z);
+    return s * fmaf(z, 1.0f - s, 1.0f);
+}
+
 }  // namespace sm100
 }  // namespace grrt_b200

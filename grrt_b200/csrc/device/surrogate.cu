@@ -10,6 +10,7 @@
 #include "integrate.cuh"
 #include "mixed_spec.cuh"
 #include "shading.cuh"
+#include "sm100.cuh"
 #include "surrogate.h"
 #include "surrogate_geom.cuh"
 
@@ -36,7 +37,7 @@ __device__ __forceinline__ unsigned fetch_work(bool want, unsigned* counter, uns
 }
 
 // the same SiLU as the tensor-core epilogues (umma_gemm.cu, mlp_fused.cu)
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return sm100::silu_fast(z); }
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ull;
@@ -522,24 +523,25 @@ __device__ __forceinline__ void add_emission(const DevScene& S, double r, double
     c[2] += e2;
 }
 
-// queue sample q for the exact re-trace (warp-aggregated)
-__device__ __forceinline__ void queue_exact(bool want, unsigned q, const DevMixedBuffers& mb) {
+// append sample q to a list (warp-aggregated over the lanes that want to)
+__device__ __forceinline__ void append(bool want, unsigned q, unsigned* count, unsigned* list) {
     const int lane = threadIdx.x & 31;
     const unsigned m = __ballot_sync(kMask, want);
     if (!m) return;
     const int leader = __ffs(m) - 1;
     unsigned base = 0;
-    if (lane == leader) base = atomicAdd(mb.retrace_count, static_cast<unsigned>(__popc(m)));
+    if (lane == leader) base = atomicAdd(count, static_cast<unsigned>(__popc(m)));
     base = __shfl_sync(kMask, base, leader);
-    if (want) mb.retrace_list[base + __popc(m & ((1u << lane) - 1u))] = q;
+    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = q;
 }
 
 __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile tile, size_t q0, size_t nq,
                              const float* __restrict__ O, const SampleAux* __restrict__ aux, RenderBands bands,
                              DevMixedBuffers mb, DevStats* stats) {
-    // whole warps stay together for the ballot in queue_exact
+    // whole warps stay together for the ballots in append
     const size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    bool exact = false;
+    bool exact = false;    // colour depends on the FP64 steps: re-trace
+    bool uncertain = false;  // the network cannot rule out the disk: FP32 speculation decides
     const unsigned q = static_cast<unsigned>(q0 + k);
     if (k < nq) {
         const SampleAux a = aux[k];
@@ -560,8 +562,11 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
                 const double r_lo = S.M / (u + du);
                 const double r_hi = (u > du) ? S.M / (u - du) : 1e30;
                 if (r_hi < S.r_in || r_lo > S.r_out) continue;  // surely outside the disk
-                if (r_lo <= S.r_in || r_hi >= S.r_out) {  // may cross an edge
-                    exact = true;
+                if (r_lo <= S.r_in || r_hi >= S.r_out) {
+                    // may cross an edge: lit or dark is the FP32 speculation's call
+                    // when the predicted radius lies outside the disk, else exact
+                    if (r < S.r_in || r > S.r_out) uncertain = true;
+                    else exact = true;
                     break;
                 }
                 double cm[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -580,7 +585,7 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
                 ++nc;
             }
         }
-        if (!exact && !captured && S.stars_on) {
+        if (!exact && !uncertain && !captured && S.stars_on) {
             const float ct = o[kOutCosTh], sp = o[kOutSinPh], cp = o[kOutCosPh];
             const float nrm = sp * sp + cp * cp;
             if (!(fabsf(ct) < 0.999f) || !(nrm > 0.5f && nrm < 2.0f)) {
@@ -600,7 +605,8 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
                 if (mixed::star_in_reach(S.stars, e, 1e-4 + bands.dir)) exact = true;
             }
         }
-        if (!exact) {
+        if (exact) uncertain = false;
+        if (!exact && !uncertain) {
             mb.sample_rgb[3 * static_cast<size_t>(q) + 0] = col[0];
             mb.sample_rgb[3 * static_cast<size_t>(q) + 1] = col[1];
             mb.sample_rgb[3 * static_cast<size_t>(q) + 2] = col[2];
@@ -608,7 +614,8 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
                 static_cast<unsigned>(captured ? kTermHorizon : kTermEscaped) | (static_cast<unsigned>(nc) << 2);
         }
     }
-    queue_exact(exact, q, mb);
+    append(exact, q, mb.retrace_count, mb.retrace_list);
+    append(uncertain, q, mb.spec_count, mb.spec_list);
     const unsigned live = __ballot_sync(kMask, k < nq);
     if ((threadIdx.x & 31) == 0 && live) atomicAdd(&stats->rays, static_cast<unsigned long long>(__popc(live)));
 }

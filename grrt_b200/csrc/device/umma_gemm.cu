@@ -42,11 +42,8 @@ struct GemmSmem {
     int failed;
 };
 
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
-__device__ __forceinline__ float silu_grad(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
-}
+__device__ __forceinline__ float silu(float z) { return sm100::silu_fast(z); }
+__device__ __forceinline__ float silu_grad(float z) { return sm100::silu_grad_fast(z); }
 
 __global__ void __launch_bounds__(kThreads, 1)
 umma_gemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_b,

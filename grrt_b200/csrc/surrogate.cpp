@@ -7,11 +7,13 @@
 // replayed. Inference: one fused tensor-core kernel (mlp_fused.cu).
 //
 // Rendering: per sample, the camera ray's closed-form margins (capture,
-// graze) and the network's outputs decide the colour; a sample whose colour
-// could move by more than the error budget under the calibrated network error
-// (disk edges, emission thresholds, stars within reach), or that lies in the
-// calibrated bands around the critical curve or a graze, is re-traced exactly
-// with the FP64 method (the mixed form's re-trace kernel), then pixels are
+// graze) and the network's outputs decide the colour. A sample whose
+// predicted crossing lies outside the disk but whose error band reaches it is
+// handed to the mixed form's FP32 speculation, which settles it as dark or
+// queues it; a sample whose colour could move by more than the error budget
+// (predicted lit, emission thresholds, stars within reach), or that lies in
+// the calibrated bands around the critical curve or a graze, is re-traced
+// exactly with the FP64 method (the mixed form's re-trace kernel); pixels are
 // resolved as in the plain form.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -495,7 +497,9 @@ struct GRRTSurrogate {
             ctx->d_mixed_scratch_bytes = bytes;
         }
         if (!ensure_inference(std::min(n, kChunk))) return false;
-        DevMixedBuffers mb = mixed_buffers(ctx->d_mixed_scratch, n, ctx->d_queue);
+        DevMixedBuffers mb = mixed_buffers_with_list(ctx->d_mixed_scratch, n, ctx->d_queue);
+        mb.r_near = ctx->mixed_r_factor * ctx->r_horizon;
+        mb.margin = ctx->mixed_margin;
         // the surrogate's kernels run on its own stream, ordered after the caller's
         cudaEvent_t e_in = nullptr;
         if (fail(cudaEventCreateWithFlags(&e_in, cudaEventDisableTiming), "event")) return false;
@@ -515,6 +519,12 @@ struct GRRTSurrogate {
             if (fail(launch_shade(S, tile, q0, nq, iO, iaux, bands, mb, ctx->d_stats, stream), "shade")) return false;
         }
         cudaEventRecord(ctx->ev_phase[1], stream);
+        // the uncertain samples: FP32 speculation (and its star pass) settles the
+        // dark ones and adds the rest to the exact list
+        if (fail(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned), stream), "memset") ||
+            fail(launch_mixed_speculate(S, tile, mb, ctx->d_stats, stream), "speculation") ||
+            fail(launch_mixed_stars(S, tile, mb, stream), "star pass"))
+            return false;
         cudaEventRecord(ctx->ev_phase[2], stream);
         if (fail(launch_mixed_retrace(S, tile, mb, ctx->d_stats, stream), "exact re-trace")) return false;
         cudaEventRecord(ctx->ev_phase[3], stream);

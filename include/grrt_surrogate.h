@@ -105,10 +105,12 @@ GRRT_EXPORT int grrt_surrogate_gradients(GRRTSurrogate* s, const float* h_in, co
 
 /* Renders the context's thin-disk frame (as grrt_render_device: d_rgba,
  * d_rgb64, d_fate may be NULL) with the surrogate: closed-form fate, network
- * crossings and escape direction, exact FP64 re-trace of the samples inside
- * the bands or whose colour is sensitive beyond tol_rel. grrt_get_stats and
+ * crossings and escape direction; the mixed form's FP32 speculation for the
+ * samples whose error band reaches the disk from outside it; exact FP64
+ * re-trace of the samples inside the bands, whose colour is sensitive beyond
+ * tol_rel, or that the speculation queues. grrt_get_stats and
  * grrt_get_phase_ms of the context report the render (phases: network +
- * shading, none, exact re-trace, resolve). */
+ * shading, speculation + star pass, exact re-trace, resolve). */
 GRRT_EXPORT int grrt_surrogate_render_device(GRRTSurrogate* s, GRRTContext* ctx, float* d_rgba, double* d_rgb64,
                                              unsigned int* d_fate, void* stream);
 GRRT_EXPORT int grrt_surrogate_render(GRRTSurrogate* s, GRRTContext* ctx, float* framebuffer);
