@@ -76,7 +76,7 @@ def parse():
     # the batched sweep (64 cameras, one persistent launch) instead of the headline frame
     ap.add_argument("--batch", action="store_true")
     # the learned surrogate (trained in this run) on its evaluation frame; 0 skips it
-    ap.add_argument("--surrogate-steps", type=int, default=8000)
+    ap.add_argument("--surrogate-steps", type=int, default=20000)
     ap.add_argument("--surrogate-size", type=int, default=2048)
     return ap.parse_args()
 
@@ -362,8 +362,8 @@ def sgemm_peak(torch) -> float:
 
 
 # One forward pass of the surrogate MLP per sample, algorithmic FLOPs:
-# 2 x (4 x 256 + 3 x 256 x 256 + 256 x 8) multiply-adds (8 outputs used).
-F_MLP = 2 * (4 * 256 + 3 * 256 * 256 + 256 * 8)
+# 2 x (4 x 256 + 3 x 256 x 256 + 256 x 9) multiply-adds (9 outputs used).
+F_MLP = 2 * (4 * 256 + 3 * 256 * 256 + 256 * 9)
 
 
 def run_surrogate(args, torch, G, stream, flush, peaks):
@@ -458,7 +458,7 @@ def run_surrogate(args, torch, G, stream, flush, peaks):
         "mlp_roofline": {"kernel": "mlp_fused_kernel", "bound": "tensor", "achieved": mlp_tflops,
                          "peak": peak, "unit": "TFLOP/s", "frac": (mlp_tflops / peak) if peak else None,
                          "launch_ms": ms_mlp, "flops_per_launch": F_MLP * rays,
-                         "flop_count": f"{F_MLP} per sample (4x256 + 3x256x256 + 256x8 multiply-adds, x2) x {rays}",
+                         "flop_count": f"{F_MLP} per sample (4x256 + 3x256x256 + 256x9 multiply-adds, x2) x {rays}",
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)"},
         "gpu_launches_per_step": 6,
     }

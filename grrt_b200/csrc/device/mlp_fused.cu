@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <cstddef>
 #include <cstdint>
 #include <mutex>
 
@@ -42,6 +43,8 @@ constexpr uint32_t kActBytes = 4 * kRows * 128;  // 4 K-blocks of 128 rows x 64 
 constexpr uint32_t kStageBytes = kHidden * 128;  // 256 rows x 64 BF16
 constexpr uint32_t kWaitLimit = 1u << 22;
 
+// FusedSmem also holds a per-CTA copy of the small parameters the epilogue
+// reads for every value (W1, b1, b2..b4, b5).
 struct FusedSmem {
     uint64_t full[kStages];
     uint64_t empty[kStages];
@@ -49,7 +52,13 @@ struct FusedSmem {
     uint64_t acc_ready;
     uint32_t tmem_base;
     int failed;
+    alignas(16) float w1[kHidden * kIn];  // read as float4 per hidden unit
+    float b1[kHidden];
+    float bh[3][kHidden];
+    float b5[kOutPad];
 };
+
+static_assert(offsetof(FusedSmem, w1) % 16 == 0, "float4 reads of W1");
 
 struct FusedMaps {
     CUtensorMap w[4];  // W2, W3, W4 (256 x 256), W5 (16 x 256)
@@ -106,6 +115,12 @@ mlp_fused_kernel(const __grid_constant__ FusedMaps maps, const float* __restrict
         sh->failed = 0;
         sm100::fence_mbar_init();
     }
+    for (int i = threadIdx.x; i < kHidden * kIn; i += blockDim.x) sh->w1[i] = params[ParamLayout::w1 + i];
+    for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+        sh->b1[i] = params[ParamLayout::b1 + i];
+        for (int l = 0; l < 3; ++l) sh->bh[l][i] = params[ParamLayout::b(l + 2) + i];
+    }
+    for (int i = threadIdx.x; i < kOutPad; i += blockDim.x) sh->b5[i] = params[ParamLayout::b5 + i];
     if (warp == kEpiWarps) {
         if (lane == 0)
             for (int l = 0; l < 4; ++l) sm100::tma_prefetch_desc(&maps.w[l]);
@@ -201,9 +216,8 @@ mlp_fused_kernel(const __grid_constant__ FusedMaps maps, const float* __restrict
                 float v[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const float* w = params + ParamLayout::w1 + (k + j) * kIn;
-                    const float z = __ldg(params + ParamLayout::b1 + k + j) + __ldg(w) * x0 + __ldg(w + 1) * x1 +
-                                    __ldg(w + 2) * x2 + __ldg(w + 3) * x3;
+                    const float4 w = *reinterpret_cast<const float4*>(&sh->w1[(k + j) * kIn]);
+                    const float z = sh->b1[k + j] + w.x * x0 + w.y * x1 + w.z * x2 + w.w * x3;
                     v[j] = silu_f(z);
                 }
                 *reinterpret_cast<uint4*>(act + act_offset(r, k)) = pack8(v);
@@ -218,14 +232,15 @@ mlp_fused_kernel(const __grid_constant__ FusedMaps maps, const float* __restrict
                 ++n_acc;
                 sm100::tc_fence_after();
                 if (l < 5) {
-                    const float* bias = params + ParamLayout::b(l);
-                    for (int k = c0; k < c0 + kHidden / 2; k += 16) {
-                        float v[16];
-                        sm100::tmem_ld16(t_row + static_cast<uint32_t>(k), v);
+                    const float* bias = sh->bh[l - 2];
+                    for (int k = c0; k < c0 + kHidden / 2; k += 32) {
+                        float v[32];
+                        sm100::tmem_ld32(t_row + static_cast<uint32_t>(k), v);
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) v[j] = silu_f(v[j] + __ldg(bias + k + j));
-                        *reinterpret_cast<uint4*>(act + act_offset(r, k)) = pack8(v);
-                        *reinterpret_cast<uint4*>(act + act_offset(r, k + 8)) = pack8(v + 8);
+                        for (int j = 0; j < 32; ++j) v[j] = silu_f(v[j] + bias[k + j]);
+#pragma unroll
+                        for (int j = 0; j < 32; j += 8)
+                            *reinterpret_cast<uint4*>(act + act_offset(r, k + j)) = pack8(v + j);
                     }
                     sm100::tc_fence_before();
                     fence_proxy_async();
@@ -238,11 +253,9 @@ mlp_fused_kernel(const __grid_constant__ FusedMaps maps, const float* __restrict
                         float* o = out + row * kOutPad;
 #pragma unroll
                         for (int j = 0; j < 16; j += 4)
-                            *reinterpret_cast<float4*>(o + j) =
-                                make_float4(v[j] + __ldg(params + ParamLayout::b5 + j),
-                                            v[j + 1] + __ldg(params + ParamLayout::b5 + j + 1),
-                                            v[j + 2] + __ldg(params + ParamLayout::b5 + j + 2),
-                                            v[j + 3] + __ldg(params + ParamLayout::b5 + j + 3));
+                            *reinterpret_cast<float4*>(o + j) = make_float4(v[j] + sh->b5[j], v[j + 1] + sh->b5[j + 1],
+                                                                            v[j + 2] + sh->b5[j + 2],
+                                                                            v[j + 3] + sh->b5[j + 3]);
                     }
                 }
             }

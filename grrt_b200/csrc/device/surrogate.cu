@@ -283,13 +283,22 @@ __global__ void loss_kernel(const float* __restrict__ O, const float* __restrict
                 const float d = o[j] - y[j];
                 l += wt * d * d;
                 gj = 2.0f * wt * d * inv;
-            } else if (j < kUsedOut && u_ok) {
+            } else if (j < kOutLogSigDir && u_ok) {
                 // log-sigma head of u slot j - kTargets: NLL with the residual fixed
                 const float d = o[j - kTargets] - y[j - kTargets];
                 const float s = fminf(fmaxf(o[j], -12.0f), 4.0f);
                 const float e = __expf(-2.0f * s);
                 l += w.sig * 0.5f * (d * d * e + 2.0f * s);
                 gj = w.sig * (1.0f - d * d * e) * inv;
+            } else if (j == kOutLogSigDir && esc) {
+                // direction head: isotropic 3-d residual of outputs 2-4
+                float d2 = 0.0f;
+#pragma unroll
+                for (int c = kOutCosTh; c <= kOutCosPh; ++c) d2 += (o[c] - y[c]) * (o[c] - y[c]);
+                const float s = fminf(fmaxf(o[j], -12.0f), 4.0f);
+                const float e = __expf(-2.0f * s);
+                l += w.sig * 0.5f * (d2 * e + 6.0f * s);
+                gj = w.sig * (3.0f - d2 * e) * inv;
             }
             g[j] = __float2bfloat16_rn(gj);
         }
@@ -588,8 +597,10 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
         if (!exact && !uncertain && !captured && S.stars_on) {
             const float ct = o[kOutCosTh], sp = o[kOutSinPh], cp = o[kOutCosPh];
             const float nrm = sp * sp + cp * cp;
+            // a star possibly in reach: the speculative pass, whose FP32
+            // trajectory gives the sky arc far more precisely, decides
             if (!(fabsf(ct) < 0.999f) || !(nrm > 0.5f && nrm < 2.0f)) {
-                exact = true;
+                uncertain = true;
             } else {
                 mixed::EscapeArc e;
                 e.th0 = acos(static_cast<double>(ct));
@@ -602,7 +613,9 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
                 const double cph = a.pph / (E * s_th * s_th);
                 e.dth = static_cast<float>(cth * du);
                 e.dph = static_cast<float>(cph * du);
-                if (mixed::star_in_reach(S.stars, e, 1e-4 + bands.dir)) exact = true;
+                const double dir_band =
+                    bands.dir * exp(fmin(fmax(static_cast<double>(o[kOutLogSigDir]), -12.0), 4.0));
+                if (mixed::star_in_reach(S.stars, e, 1e-4 + dir_band)) uncertain = true;
             }
         }
         if (exact) uncertain = false;
@@ -646,8 +659,9 @@ __global__ void eval_errors_kernel(const float* __restrict__ O, const float* __r
         const float px = st_p * o[4] * np, py = st_p * o[3] * np, pz = o[2];
         const float tx = st_t * y[4], ty = st_t * y[3], tz = y[2];
         const float dx = px - tx, dy = py - ty, dz = pz - tz;
-        e[2] = 2.0f * asinf(fminf(1.0f, 0.5f * sqrtf(dx * dx + dy * dy + dz * dz)));
-        e[3] = fabsf(o[5] - y[5]) / static_cast<float>(kCThScale);
+        const float inv_sig = __expf(-fminf(fmaxf(o[kOutLogSigDir], -12.0f), 4.0f));
+        e[2] = 2.0f * asinf(fminf(1.0f, 0.5f * sqrtf(dx * dx + dy * dy + dz * dz))) * inv_sig;
+        e[3] = fabsf(o[5] - y[5]) / static_cast<float>(kCThScale) * inv_sig;
     } else {
         e[2] = e[3] = -1.0f;
     }

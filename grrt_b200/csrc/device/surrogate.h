@@ -18,7 +18,7 @@ namespace surr {
 constexpr int kIn = 4;
 constexpr int kHidden = 256;
 constexpr int kTargets = 6;   // fitted quantities (u1, u2, cos theta, sin phi, cos phi, c_theta)
-constexpr int kUsedOut = 8;   // outputs: the targets, then log sigma of the u1 and u2 errors
+constexpr int kUsedOut = 9;   // outputs: the targets, then log sigma of the u1, u2 and direction errors
 constexpr int kOutPad = 16;   // output layer rows computed by the GEMM (kUsedOut used)
 constexpr int kDOutPad = 64;  // K of the output layer's backward GEMM
 constexpr int kYCols = 10;    // 6 targets, termination, later crossings, capture margin, graze margin
@@ -45,8 +45,9 @@ struct ParamLayout {
 };
 
 // Loss weights: squared error of the six targets, and the Gaussian negative
-// log-likelihood 0.5 (d^2 exp(-2 s) + 2 s) of the two log-sigma heads, with
-// the u residual d held fixed (the heads learn the error, not the value).
+// log-likelihood of the log-sigma heads with the residual held fixed (the
+// heads learn the error, not the value): 0.5 (d^2 exp(-2 s) + 2 s) for u1 and
+// u2, 0.5 (|d|^2 exp(-2 s) + 6 s) for the three direction outputs.
 struct LossWeights {
     float u = 16.0f, dir = 0.5f, cth = 0.25f, sig = 0.1f;
 };
@@ -92,7 +93,7 @@ cudaError_t launch_cast_weights(const float* params, __nv_bfloat16* const* wb, _
 // place in the exact re-trace queue.
 struct RenderBands {
     double du = 4.0;           // u error band = du * sigma (the sample's predicted error)
-    double dir = 1e-3;         // calibrated escape-direction error (rad)
+    double dir = 4.0;          // direction error band (rad) = dir * sigma_dir
     double capture = 0.15;     // |capture margin| below this: exact
     double graze = 0.02;       // graze margin below this: exact
     double tol_rel = 1e-3;     // colour sensitivity budget (relative)
@@ -109,7 +110,8 @@ cudaError_t launch_shade(const DevScene& S, const DevTile& tile, size_t q0, size
 
 // Validation: per sample, errors of the network outputs against the targets
 // (err[q][0] = |du1| / sigma1, [1] = |du2| / sigma2, [2] = arc-start direction
-// error (rad), [3] = |c_theta error|; -1 where the target does not apply).
+// error (rad) / sigma_dir, [3] = |c_theta error| / sigma_dir; -1 where the
+// target does not apply).
 cudaError_t launch_eval_errors(const float* O, const float* Y, size_t n, float* err, cudaStream_t s);
 
 }  // namespace surr

@@ -123,11 +123,12 @@ GRRT_HD void encode_inputs(double alpha, double beta, double spin, double incl, 
     out[3] = static_cast<float>((incl - 47.5 * kDeg) / (42.5 * kDeg));
 }
 
-// Output slots of the network (8 used of the 16 the last GEMM computes): the
-// six quantities, then log sigma of the network's own error on u1 and u2.
+// Output slots of the network (9 used of the 16 the last GEMM computes): the
+// six quantities, then log sigma of the network's own error on u1, u2 and on
+// the sky direction (outputs 2-4).
 enum : int {
     kOutU1 = 0, kOutU2 = 1, kOutCosTh = 2, kOutSinPh = 3, kOutCosPh = 4, kOutCTh = 5,
-    kOutLogSig1 = 6, kOutLogSig2 = 7, kOutputs = 8
+    kOutLogSig1 = 6, kOutLogSig2 = 7, kOutLogSigDir = 8, kOutputs = 9
 };
 constexpr double kCThScale = 1.0 / 32.0;  // c_theta = r^2 dtheta/dr is O(b) ~ tens of M
 

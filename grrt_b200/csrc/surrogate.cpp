@@ -621,6 +621,8 @@ struct GRRTSurrogate {
         const double median_du = quantile(du, 0.5);
         bands.du = safety * quantile(du, q);  // multiple of the predicted sigma
         const double du_arc = 1.0 / 1000.0 - 1.0 / 7000.0;
+        // direction: multiple of sigma_dir covering the arc-start error and the
+        // arc-length error from c_theta
         bands.dir = safety * (quantile(dir, q) + quantile(cth, q) * du_arc);
         bands.capture = cap_band;
         bands.graze = kFitGraze;

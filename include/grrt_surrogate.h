@@ -41,9 +41,10 @@ GRRT_EXPORT int grrt_surrogate_gemm_bf16(const void* A, int lda, const void* B, 
  *   2-4:  cos(theta), sin(phi), cos(phi) of the sky position at r = 1000 M
  *         (folded as the star lookup folds it)
  *   5:    c_theta / 32 with c_theta = r^2 dtheta/dr there (far-field bending)
- *   6, 7: log sigma of the network's own error on outputs 0 and 1, trained by
- *         a Gaussian likelihood on the residual; a sample's u band is a
- *         calibrated multiple of its sigma.
+ *   6, 7: log sigma of the network's own error on outputs 0 and 1, and
+ *   8:    on the direction (outputs 2-4), trained by a Gaussian likelihood on
+ *         the residual; a sample's u and direction bands are calibrated
+ *         multiples of its sigmas.
  * The redshift factor g is not learned: at a crossing radius it follows in
  * closed form from the ray's constants (p_t, p_phi), as in the plain form. */
 typedef struct GRRTSurrogate GRRTSurrogate;
@@ -78,7 +79,7 @@ GRRT_EXPORT int grrt_surrogate_train(GRRTSurrogate* s, int steps, int batch, dou
  * Graze band: turning point within mu = 0.02 of the equator. u band: the
  * `quantile` of |u error| / sigma over the samples outside both bands, times
  * `safety` (a multiple of each sample's predicted sigma); direction band: the
- * `quantile` of the direction error times `safety`. report8 (or NULL): u band
+ * same for the direction error over sigma_dir. report8 (or NULL): u band
  * multiple, direction band, capture band, graze band, validation samples,
  * fate disagreements, fraction of samples in the bands, median |u error| /
  * sigma outside them. */
@@ -91,7 +92,7 @@ GRRT_EXPORT int grrt_surrogate_set_bands(GRRTSurrogate* s, double du, double dir
 GRRT_EXPORT int grrt_surrogate_get_bands(const GRRTSurrogate* s, double* out5);
 
 /* FP32 parameters: W1[256x4], b1, W2..W4[256x256], b2..b4, W5[16x256]
- * (rows 8..15 zero), b5[16]. Returns the count; copies when capacity allows. */
+ * (rows 9..15 zero), b5[16]. Returns the count; copies when capacity allows. */
 GRRT_EXPORT long long grrt_surrogate_params(GRRTSurrogate* s, float* out, long long capacity);
 GRRT_EXPORT int grrt_surrogate_set_params(GRRTSurrogate* s, const float* in, long long n);
 /* Network outputs float[n][16] for device inputs float[n][4] (the fused
@@ -106,7 +107,8 @@ GRRT_EXPORT int grrt_surrogate_gradients(GRRTSurrogate* s, const float* h_in, co
 /* Renders the context's thin-disk frame (as grrt_render_device: d_rgba,
  * d_rgb64, d_fate may be NULL) with the surrogate: closed-form fate, network
  * crossings and escape direction; the mixed form's FP32 speculation for the
- * samples whose error band reaches the disk from outside it; exact FP64
+ * samples whose error band reaches the disk from outside it or whose sky arc
+ * (widened by the direction band) could reach a star; exact FP64
  * re-trace of the samples inside the bands, whose colour is sensitive beyond
  * tol_rel, or that the speculation queues. grrt_get_stats and
  * grrt_get_phase_ms of the context report the render (phases: network +

@@ -14,7 +14,7 @@ import numpy as np
 HID = 256
 OUT_PAD = 16
 USED = 6      # fitted targets
-HEADS = 8     # outputs used: targets + log-sigma heads of u1, u2
+HEADS = 9     # outputs used: targets + log-sigma heads of u1, u2, direction
 WEIGHTS = {"u": 16.0, "dir": 0.5, "cth": 0.25, "sig": 0.1}  # surr::LossWeights
 FIT_CAPTURE, FIT_GRAZE = 0.05, 0.02  # surr::kFitCapture, kFitGraze
 
@@ -93,12 +93,18 @@ def loss_terms(o, Y):
     loss = np.sum(w * d * d)
     g = 2.0 * w * d
     u_ok = w[:, 0] > 0
+    esc = w[:, 2] > 0
     for j in (6, 7):
         s = np.clip(o[:, j], -12.0, 4.0)
         e = np.exp(-2.0 * s)
         dj = d[:, j - 6]
         loss += np.sum(np.where(u_ok, WEIGHTS["sig"] * 0.5 * (dj * dj * e + 2.0 * s), 0.0))
         g[:, j] = np.where(u_ok, WEIGHTS["sig"] * (1.0 - dj * dj * e), 0.0)
+    s = np.clip(o[:, 8], -12.0, 4.0)
+    e = np.exp(-2.0 * s)
+    d2 = np.sum(d[:, 2:5] ** 2, axis=1)
+    loss += np.sum(np.where(esc, WEIGHTS["sig"] * 0.5 * (d2 * e + 6.0 * s), 0.0))
+    g[:, 8] = np.where(esc, WEIGHTS["sig"] * (3.0 - d2 * e), 0.0)
     return float(loss / B), g / B
 
 

@@ -44,14 +44,15 @@ def test_bf16_rounding_is_round_to_nearest_even():
 
 
 def test_sigma_head_gradient_matches_finite_differences():
-    """The log-sigma heads (rows 6, 7 of W5 and b5) see the u residual as a
-    constant: their own parameters' gradients are finite differences of the loss."""
+    """The log-sigma heads (rows 6-8 of W5 and b5) see their residuals as
+    constants: their own parameters' gradients are finite differences of the loss."""
     p = mlp_ref.random_params(11)
     X, Y = mlp_ref.random_batch(12, 32)
     _, g = mlp_ref.loss_and_grads(p, X, Y, bf=False)
     w5 = 256 * 4 + 256 + 3 * (65536 + 256)
     b5 = w5 + 16 * 256
-    idx = [w5 + 6 * 256 + k for k in (0, 17, 255)] + [w5 + 7 * 256 + k for k in (3, 100)] + [b5 + 6, b5 + 7]
+    idx = ([w5 + 6 * 256 + k for k in (0, 17, 255)] + [w5 + 7 * 256 + k for k in (3, 100)] +
+           [w5 + 8 * 256 + k for k in (5, 200)] + [b5 + 6, b5 + 7, b5 + 8])
     for i in idx:
         h = 1e-6
         pp, pm = p.copy(), p.copy()
