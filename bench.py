@@ -261,6 +261,33 @@ def run_batch(args):
         torch.cuda.synchronize()
         sep.append(e0.elapsed_time(e1))
     sep_ms = float(np.mean(sep))
+    mixed_vs_fp64 = None
+    if form == G.FORM_MIXED:
+        # the same batch in the FP64 form: time, and the mixed images' error
+        got = out.cpu().numpy()
+        B64 = G.Batch(cams)
+        B64.autotune(cache)
+        out64 = torch.empty_like(out)
+        for _ in range(max(1, args.warmup)):
+            B64.render_device(out64, stream)
+        torch.cuda.synchronize()
+        t64 = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                B64.render_device(out64, stream)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            t64.append(e0.elapsed_time(e1))
+        ref = out64.cpu().numpy()
+        scale = float(ref[:, :3].max())
+        rel = np.abs(got[:, :3] - ref[:, :3]) / np.maximum(np.abs(ref[:, :3]), 1e-6 * scale)
+        mixed_vs_fp64 = {"fp64_batch_ms": float(np.mean(t64)), "speedup": float(np.mean(t64)) / ms,
+                         "max_rel_err": float(rel.max()), "pixels_above_1e-4": int(np.sum(rel.max(axis=1) > 1e-4)),
+                         "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])}
+        B64.close()
     chunk, order, bps = B.schedule()
     line = {"metric": "batched sweep rays/s (64 Kerr cameras x 256^2, one persistent launch)", "value": rays / (ms * 1e-3),
             "unit": "rays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -270,7 +297,11 @@ def run_batch(args):
                                                            "blocks_per_sm": bps, "autotune_ms": tuned_ms},
                        "l2": "flushed between steps"},
             "separate_launches_ms_per_step": sep_ms, "batched_speedup": sep_ms / ms,
-            "work": {"attempts_per_ray": st["attempts"] / max(1, st["rays"])}, "gpu_launches": args.steps}
+            "work": {"attempts_per_ray": st["attempts"] / max(1, st["rays"])},
+            # FP64: one persistent launch; mixed: speculate, stars, re-trace, resolve
+            "gpu_launches": args.steps * (4 if form == G.FORM_MIXED else 1)}
+    if mixed_vs_fp64 is not None:
+        line["mixed_vs_fp64_batch"] = mixed_vs_fp64
     print(json.dumps(line), flush=True)
 
 

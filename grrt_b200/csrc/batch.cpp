@@ -5,6 +5,11 @@
 // descriptions sit in one device array. An autotuner times candidate schedules
 // (chunk size, chunk order across cameras, resident blocks per SM) and keeps
 // the fastest, optionally caching the choice in a JSON file.
+//
+// In the mixed form the batch runs the mixed pipeline (FP32 speculation, star
+// pass, FP64 re-trace, resolve) with each phase one launch over the samples
+// of all cameras; the graph holds the four launches. Its phases take samples
+// in camera order, so of the schedule only the resident blocks per SM apply.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +32,8 @@ struct GRRTBatch {
     std::vector<std::unique_ptr<GRRTContext>> cams;
     std::vector<DevBatchItem> items;
     size_t total_pixels = 0;
+    size_t total_samples = 0;  // mixed form's sample space (set with the device state)
+    bool any_stars = false;
     int form = GRRT_FORM_FP64;
     // schedule
     int chunk_size = 256;
@@ -43,6 +50,8 @@ struct GRRTBatch {
     unsigned* d_queue = nullptr;
     DevStats* d_stats = nullptr;
     float4* d_out = nullptr;  // output of the host-buffer entry point
+    void* d_mixed = nullptr;  // mixed form's scratch
+    size_t mixed_bytes = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -60,6 +69,7 @@ struct GRRTBatch {
         cudaFree(d_queue);
         cudaFree(d_stats);
         cudaFree(d_out);
+        cudaFree(d_mixed);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -121,14 +131,21 @@ struct GRRTBatch {
         B.chunks = d_chunks;
         B.n_chunks = n_chunks;
         B.chunk_size = chunk_size;
+        B.n_items = static_cast<int>(items.size());
+        B.n_samples = static_cast<unsigned>(total_samples);
+        B.n_pixels = total_pixels;
         return B;
+    }
+
+    static int max_blocks_per_sm(int f) {
+        return f == GRRT_FORM_MIXED ? mixed_batch_max_blocks_per_sm() : thin_batch_max_blocks_per_sm();
     }
 
     int blocks() const {
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int maxb = thin_batch_max_blocks_per_sm(form);
+        const int maxb = max_blocks_per_sm(form);
         const int per = (blocks_per_sm > 0 && blocks_per_sm < maxb) ? blocks_per_sm : maxb;
         return sms * per;
     }
@@ -137,13 +154,33 @@ struct GRRTBatch {
     int launch(float4* out, cudaStream_t s) {
         if (!upload_schedule()) return -1;
         const int nb = blocks();
+        const bool mixed = form == GRRT_FORM_MIXED;
+        if (mixed) {
+            if (total_samples > 0xffffffffull) {
+                error = "the mixed form indexes samples in 32 bits; this batch has " + std::to_string(total_samples);
+                return -1;
+            }
+            const size_t need = mixed_scratch_bytes_for(total_samples);
+            if (need > mixed_bytes) {
+                if (graph) cudaGraphExecDestroy(graph);
+                graph = nullptr;
+                cudaFree(d_mixed);
+                d_mixed = nullptr;
+                mixed_bytes = 0;
+                if (fail(cudaMalloc(&d_mixed, need), "cudaMalloc(mixed scratch)")) return -1;
+                mixed_bytes = need;
+            }
+        }
         if (!graph || graph_out != out || graph_form != form || graph_blocks != nb) {
             if (graph) cudaGraphExecDestroy(graph);
             graph = nullptr;
             cudaGraph_t g = nullptr;
             if (fail(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return -1;
             cudaMemsetAsync(d_stats, 0, sizeof(DevStats), stream);
-            const cudaError_t le = launch_thin_batch(desc(), out, d_queue, d_stats, form, nb, stream);
+            const cudaError_t le =
+                mixed ? launch_thin_mixed_batch(desc(), any_stars, out, d_queue, d_stats, d_mixed, mixed_bytes,
+                                                blocks_per_sm, stream)
+                      : launch_thin_batch(desc(), out, d_queue, d_stats, nb, stream);
             const cudaError_t ce = cudaStreamEndCapture(stream, &g);
             if (fail(le, "batch launch") || fail(ce, "end capture")) {
                 if (g) cudaGraphDestroy(g);
@@ -237,6 +274,16 @@ static bool batch_ensure_device(GRRTBatch* b) {
         scenes.push_back(c->scene_for_launch());
     }
     b->device = b->cams[0]->device;
+    // the mixed form's sample space: each item's samples (pixel-major, grid^2
+    // per pixel) after those of the items before it
+    size_t s0 = 0;
+    for (auto& it : b->items) {
+        const DevScene& sc = scenes[static_cast<size_t>(it.scene)];
+        it.sample0 = s0;
+        s0 += static_cast<size_t>(it.w) * it.h * static_cast<size_t>(sc.grid) * static_cast<size_t>(sc.grid);
+        b->any_stars = b->any_stars || sc.stars_on != 0;
+    }
+    b->total_samples = s0;
     if (b->fail(cudaMalloc(&b->d_scenes, sizeof(DevScene) * scenes.size()), "cudaMalloc(scenes)")) return false;
     if (b->fail(cudaMemcpy(b->d_scenes, scenes.data(), sizeof(DevScene) * scenes.size(), cudaMemcpyHostToDevice),
                 "upload scenes"))
@@ -256,6 +303,7 @@ static bool batch_ensure_device(GRRTBatch* b) {
 extern "C" GRRT_EXPORT int grrt_batch_set_precision(GRRTBatch* b, int form) {
     if (!b || (form != GRRT_FORM_FP64 && form != GRRT_FORM_MIXED)) return -1;
     if (form == b->form) return 0;
+
     b->form = form;
     if (b->d_scenes) {
         // scenes carry the form's knobs; re-upload
@@ -364,11 +412,16 @@ extern "C" GRRT_EXPORT int grrt_batch_autotune(GRRTBatch* b, const char* cache_p
         }
     }
     if (!b->d_out && b->fail(cudaMalloc(&b->d_out, sizeof(float4) * b->total_pixels), "cudaMalloc(output)")) return -1;
-    const int maxb = thin_batch_max_blocks_per_sm(b->form);
+    const int maxb = GRRTBatch::max_blocks_per_sm(b->form);
     double best = 1e30;
     int bc = b->chunk_size, bo = b->order, bb = b->blocks_per_sm;
-    for (int order : {GRRT_BATCH_ORDER_ROUND_ROBIN, GRRT_BATCH_ORDER_CAMERA_MAJOR})
-        for (int cs : {64, 256, 1024, 4096})
+    // the mixed form's phases ignore the chunk table: only the occupancy varies
+    const bool mixed = b->form == GRRT_FORM_MIXED;
+    const std::vector<int> orders = mixed ? std::vector<int>{b->order}
+                                          : std::vector<int>{GRRT_BATCH_ORDER_ROUND_ROBIN, GRRT_BATCH_ORDER_CAMERA_MAJOR};
+    const std::vector<int> chunks = mixed ? std::vector<int>{b->chunk_size} : std::vector<int>{64, 256, 1024, 4096};
+    for (int order : orders)
+        for (int cs : chunks)
             for (int bp : {maxb, std::max(1, maxb - 1)}) {
                 grrt_batch_set_schedule(b, cs, order, bp);
                 double t = 1e30;

@@ -285,6 +285,7 @@ DevScene GRRTContext::scene_for_launch() const {
     DevScene S = dev;
     S.fp32_r_min = mixed_r_factor * r_horizon;
     S.tol_fp32 = tol_fp32;
+    S.mixed_margin = mixed_margin;
     return S;
 }
 
@@ -342,7 +343,7 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
         e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
                               mixed_r_factor * r_horizon, ev_phase, s);
     else
-        e = launch_thin(S, tile, out, res, form, s);
+        e = launch_thin(S, tile, out, res, s);
     cudaEventRecord(ev1, s);
     n_phases = mixed_thin ? kMixedPhases : 0;
     if (fail_cuda(e, "render launch")) return -1;

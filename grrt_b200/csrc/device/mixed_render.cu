@@ -14,6 +14,11 @@
 //     form's arithmetic, lanes pulling from the queue (converged FP64 warps).
 //   resolve: per pixel, the spp samples are summed in order and scaled, as
 //     Renderer::render does (src/renderer.cpp:47-72).
+//
+// The batched form runs the same four phases over the samples of many
+// cameras at once (one sample space, items in order), so each phase is one
+// launch for the whole batch and every sample gets the arithmetic of its own
+// camera's single render.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -42,6 +47,39 @@ __device__ __forceinline__ void sample_start(const DevScene& S, const DevTile& t
     y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], p[1], p[2]};
     pt = p[0];
     pph = p[3];
+}
+
+// Batch item holding sample q (kBySample) or output pixel q: the last item
+// whose first sample (first pixel) is <= q; items are stored in that order.
+template <bool kBySample>
+__device__ __forceinline__ const DevBatchItem& batch_item(const DevBatch& B, size_t q) {
+    int lo = 0, hi = B.n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const size_t first = kBySample ? B.items[mid].sample0 : B.items[mid].out_offset;
+        if (first <= q)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return B.items[lo];
+}
+
+// Camera ray of sample q. One camera: q indexes the tile's samples (pixel-major,
+// spp samples per pixel). Batch: q indexes the samples of all items in item
+// order, and the lane's scene becomes the item's.
+template <bool kBatch>
+__device__ __forceinline__ void start_ray(const DevScene& S0, const DevTile& tile, const DevBatch& B, unsigned q,
+                                          const DevScene*& sp, Vec5<double>& y, double& pt, double& pph) {
+    if (kBatch) {
+        const DevBatchItem& it = batch_item<true>(B, q);
+        const DevTile t{it.x0, it.y0, it.w, it.h, it.out_pitch};
+        const unsigned local = static_cast<unsigned>(q - it.sample0);
+        sp = B.scenes + it.scene;
+        sample_start(*sp, t, local, sp->grid * sp->grid, y, pt, pph);
+    } else {
+        sample_start(S0, tile, q, S0.grid * S0.grid, y, pt, pph);
+    }
 }
 
 // Queues sample q for the FP64 re-trace (warp-aggregated over the lanes that ask).
@@ -97,11 +135,22 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 
 }  // namespace
 
+// Every kernel below comes in two instantiations: kBatch = false renders the
+// tile of one camera (scene S0, a kernel parameter); kBatch = true renders
+// every item of the batch B (scenes in global memory, one per lane's sample),
+// over one sample space, so one launch per phase covers all cameras.
+// Inside, S names the scene of the lane's current sample.
+
+template <bool kBatch>
 __global__ void __launch_bounds__(kMixThreads, 4)
-mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb, DevStats* stats) {
-    const int g2 = S.grid * S.grid;
-    const unsigned total = mb.spec_list ? *mb.spec_count : static_cast<unsigned>(tile.w) * tile.h * g2;
-    const float Mf = static_cast<float>(S.M), af = static_cast<float>(S.a);
+mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
+                       DevMixedBuffers mb, DevStats* stats) {
+    const DevScene* sp = nullptr;
+#define S (kBatch ? *sp : S0)
+    const unsigned total = kBatch ? B.n_samples
+                                  : (mb.spec_list ? *mb.spec_count
+                                                  : static_cast<unsigned>(tile.w) * tile.h * (S0.grid * S0.grid));
+    float Mf = static_cast<float>(S0.M), af = static_cast<float>(S0.a);
     unsigned long long n_att = 0, n_acc = 0, n_rays = 0;
     unsigned q = ~0u;
     bool live = false, exhausted = false;
@@ -116,12 +165,19 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, D
             if (nq == ~0u) {
                 exhausted = true;
             } else {
-                q = mb.spec_list ? mb.spec_list[nq] : nq;
-                sample_start(S, tile, q, g2, y, pt, pph);
+                q = (!kBatch && mb.spec_list) ? mb.spec_list[nq] : nq;
+                start_ray<kBatch>(S0, tile, B, q, sp, y, pt, pph);
+                if (kBatch) {
+                    Mf = static_cast<float>(S.M);
+                    af = static_cast<float>(S.a);
+                }
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
-                trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near);
+                if (kBatch)
+                    trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.fp32_r_min);
+                else
+                    trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near);
                 live = true;
             }
         }
@@ -152,7 +208,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, D
         bool queue = false;
         if (live && term >= 0) {
             live = false;
-            if (!mb.spec_list) ++n_rays;  // a list's samples are counted by its producer
+            if (kBatch || !mb.spec_list) ++n_rays;  // a list's samples are counted by its producer
             const size_t o = 3 * static_cast<size_t>(q);
             if (retrace || term == kTermMaxSteps) {
                 queue = true;
@@ -174,19 +230,23 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, D
         }
         queue_retrace(queue, q, mb);
     }
+#undef S
     warp_add(stats, n_att, n_acc, n_rays, 0ull);
 }
 
 // Star pass over the pending escapes: colour 0, or queued for the re-trace.
+template <bool kBatch>
 __global__ void __launch_bounds__(256)
-mixed_star_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb) {
-    const unsigned n = static_cast<unsigned>(tile.w) * tile.h * (S.grid * S.grid);
+mixed_star_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
+                  DevMixedBuffers mb) {
+    const unsigned n = kBatch ? B.n_samples : static_cast<unsigned>(tile.w) * tile.h * (S0.grid * S0.grid);
     const unsigned stride = gridDim.x * blockDim.x;
     // whole warps iterate together so queue_retrace can ballot
     for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const unsigned q = base + threadIdx.x;
         bool queue = false;
         if (q < n && mb.sample_fate[q] == mixed::kFateStarPending) {
+            const DevScene& S = kBatch ? B.scenes[batch_item<true>(B, q).scene] : S0;
             const size_t o = 3 * static_cast<size_t>(q);
             mixed::EscapeArc e;
             e.th0 = mb.sample_rgb[o + 0];
@@ -208,9 +268,12 @@ mixed_star_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMix
 }
 
 // FP64 re-trace of the queued samples with the plain form's arithmetic.
+template <bool kBatch>
 __global__ void __launch_bounds__(kMixThreads, 4)
-mixed_retrace_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb, DevStats* stats) {
-    const int g2 = S.grid * S.grid;
+mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
+                     DevMixedBuffers mb, DevStats* stats) {
+    const DevScene* sp = nullptr;
+#define S (kBatch ? *sp : S0)
     const unsigned total = *mb.retrace_count;
     unsigned long long n_att = 0, n_acc = 0;
     unsigned q = ~0u;
@@ -227,7 +290,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S, const DevTile tile, Dev
                 exhausted = true;
             } else {
                 q = mb.retrace_list[nq];
-                sample_start(S, tile, q, g2, y, pt, pph);
+                start_ray<kBatch>(S0, tile, B, q, sp, y, pt, pph);
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
@@ -287,20 +350,39 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S, const DevTile tile, Dev
             mb.sample_fate[q] = static_cast<unsigned>(term) | (nc << 2);
         }
     }
+#undef S
     warp_add(stats, n_att, n_acc, 0ull, n_att);
 }
 
 // Per pixel: sum the spp sample colours in order, scale, write the outputs.
-__global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S, const DevTile tile, DevMixedBuffers mb,
+template <bool kBatch>
+__global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S0, const DevTile tile,
+                                     const __grid_constant__ DevBatch B, DevMixedBuffers mb,
                                      float4* __restrict__ out_rgba, double* __restrict__ out_rgb64,
                                      uint32_t* __restrict__ out_fate, DevStats* stats) {
-    const int g2 = S.grid * S.grid;
-    const unsigned npix = static_cast<unsigned>(tile.w) * tile.h;
+    const size_t npix = kBatch ? B.n_pixels : static_cast<size_t>(tile.w) * tile.h;
     unsigned long long hz = 0, es = 0, mx = 0, cr = 0;
-    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < npix;
+         p += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const DevScene* sp = &S0;
+        size_t q0, o;
+        if (kBatch) {
+            const DevBatchItem& it = batch_item<false>(B, p);
+            sp = B.scenes + it.scene;
+            const size_t local = p - it.out_offset;
+            q0 = it.sample0 + local * static_cast<size_t>(sp->grid * sp->grid);
+            const int qx = static_cast<int>(local % it.w), qy = static_cast<int>(local / it.w);
+            o = it.out_offset + static_cast<size_t>(qy) * it.out_pitch + qx;
+        } else {
+            q0 = p * static_cast<size_t>(S0.grid * S0.grid);
+            const int qx = static_cast<int>(p % tile.w), qy = static_cast<int>(p / tile.w);
+            o = static_cast<size_t>(qy) * tile.out_pitch + qx;
+        }
+        const DevScene& S = kBatch ? *sp : S0;
+        const int g2 = S.grid * S.grid;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
         for (int s = 0; s < g2; ++s) {
-            const size_t q = static_cast<size_t>(p) * g2 + s;
+            const size_t q = q0 + s;
             a0 = a0 + mb.sample_rgb[3 * q + 0];
             a1 = a1 + mb.sample_rgb[3 * q + 1];
             a2 = a2 + mb.sample_rgb[3 * q + 2];
@@ -312,8 +394,6 @@ __global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S, const D
             cr += f >> 2;
             if (out_fate) out_fate[q] = f;
         }
-        const int qx = static_cast<int>(p % tile.w), qy = static_cast<int>(p / tile.w);
-        const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
         const double r0 = a0 * S.inv_spp, r1 = a1 * S.inv_spp, r2 = a2 * S.inv_spp;
         if (out_rgba)
             out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1), static_cast<float>(r2), 1.0f);
@@ -338,14 +418,19 @@ __global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S, const D
     }
 }
 
+size_t mixed_scratch_bytes_for(size_t n_samples) {
+    return n_samples * (3 * sizeof(double) + 3 * sizeof(unsigned)) + 1024;
+}
+
 size_t mixed_scratch_bytes(const DevTile& tile, int g2) {
-    const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
-    return n * (3 * sizeof(double) + 3 * sizeof(unsigned)) + 1024;
+    return mixed_scratch_bytes_for(static_cast<size_t>(tile.w) * tile.h * g2);
 }
 
 namespace {
 struct MixLaunchShape {
-    int sms = 0, per_spec = 1, per_retrace = 1;
+    int sms = 0;
+    int per_spec = 1, per_retrace = 1;      // resident blocks per SM, one camera
+    int per_spec_b = 1, per_retrace_b = 1;  // the batch instantiations
 };
 const MixLaunchShape& mix_shape() {
     static MixLaunchShape sh;
@@ -353,10 +438,14 @@ const MixLaunchShape& mix_shape() {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sh.sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, mixed_speculate_kernel, kMixThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, mixed_retrace_kernel, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, mixed_speculate_kernel<false>, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, mixed_retrace_kernel<false>, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec_b, mixed_speculate_kernel<true>, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace_b, mixed_retrace_kernel<true>, kMixThreads, 0);
         if (sh.per_spec < 1) sh.per_spec = 1;
         if (sh.per_retrace < 1) sh.per_retrace = 1;
+        if (sh.per_spec_b < 1) sh.per_spec_b = 1;
+        if (sh.per_retrace_b < 1) sh.per_retrace_b = 1;
     }
     return sh;
 }
@@ -386,8 +475,9 @@ cudaError_t launch_mixed_speculate(const DevScene& S, const DevTile& tile, const
     const MixLaunchShape& sh = mix_shape();
     const size_t n = static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid;
     const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
-    mixed_speculate_kernel<<<need < sh.sms * sh.per_spec ? need : sh.sms * sh.per_spec, kMixThreads, 0, stream>>>(
-        S, tile, mb, stats);
+    mixed_speculate_kernel<false>
+        <<<need < sh.sms * sh.per_spec ? need : sh.sms * sh.per_spec, kMixThreads, 0, stream>>>(S, tile, DevBatch{},
+                                                                                                  mb, stats);
     return cudaGetLastError();
 }
 
@@ -398,14 +488,14 @@ cudaError_t launch_mixed_stars(const DevScene& S, const DevTile& tile, const Dev
     const size_t n = static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid;
     int sb = static_cast<int>((n + 255) / 256);
     if (sb > sh.sms * 8) sb = sh.sms * 8;
-    mixed_star_kernel<<<sb, 256, 0, stream>>>(S, tile, mb);
+    mixed_star_kernel<false><<<sb, 256, 0, stream>>>(S, tile, DevBatch{}, mb);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
                                  cudaStream_t stream) {
     const MixLaunchShape& sh = mix_shape();
-    mixed_retrace_kernel<<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, mb, stats);
+    mixed_retrace_kernel<false><<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, mb, stats);
     return cudaGetLastError();
 }
 
@@ -416,7 +506,8 @@ cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const D
     int rb = static_cast<int>((npix + 255) / 256);
     if (rb > sh.sms * 8) rb = sh.sms * 8;
     if (rb < 1) rb = 1;
-    mixed_resolve_kernel<<<rb, 256, 0, stream>>>(S, tile, mb, out.rgba, out.rgb64, out.fate, stats);
+    mixed_resolve_kernel<false>
+        <<<rb, 256, 0, stream>>>(S, tile, DevBatch{}, mb, out.rgba, out.rgb64, out.fate, stats);
     return cudaGetLastError();
 }
 
@@ -439,21 +530,12 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
-    const MixLaunchShape& sh = mix_shape();
-    const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
     mark(0);
-    mixed_speculate_kernel<<<need < sh.sms * sh.per_spec ? need : sh.sms * sh.per_spec, kMixThreads, 0, stream>>>(
-        S, tile, mb, stats);
-    e = cudaGetLastError();
+    e = launch_mixed_speculate(S, tile, mb, stats, stream);
     if (e != cudaSuccess) return e;
     mark(1);
-    if (S.stars_on) {
-        int sb = static_cast<int>((n + 255) / 256);
-        if (sb > sh.sms * 8) sb = sh.sms * 8;
-        mixed_star_kernel<<<sb, 256, 0, stream>>>(S, tile, mb);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
+    e = launch_mixed_stars(S, tile, mb, stream);
+    if (e != cudaSuccess) return e;
     mark(2);
     e = launch_mixed_retrace(S, tile, mb, stats, stream);
     if (e != cudaSuccess) return e;
@@ -461,6 +543,47 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     e = launch_mixed_resolve(S, tile, mb, out, stats, stream);
     mark(4);
     return e;
+}
+
+int mixed_batch_max_blocks_per_sm() { return mix_shape().per_spec_b; }
+
+cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* out_rgba, unsigned* queue,
+                                    DevStats* stats, void* scratch, size_t scratch_bytes, int blocks_per_sm,
+                                    cudaStream_t stream) {
+    const size_t n = B.n_samples;
+    if (n == 0) return cudaSuccess;
+    if (B.n_items < 1 || scratch_bytes < mixed_scratch_bytes_for(n)) return cudaErrorInvalidValue;
+    const DevMixedBuffers mb = mixed_buffers(scratch, n, queue);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 1024, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(queue, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const MixLaunchShape& sh = mix_shape();
+    auto per = [&](int maxb) { return (blocks_per_sm > 0 && blocks_per_sm < maxb) ? blocks_per_sm : maxb; };
+    const DevScene none{};
+    const DevTile no_tile{};
+    const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
+    int sb = sh.sms * per(sh.per_spec_b);
+    if (need < sb) sb = need;
+    mixed_speculate_kernel<true><<<sb, kMixThreads, 0, stream>>>(none, no_tile, B, mb, stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (any_stars) {
+        int b = static_cast<int>((n + 255) / 256);
+        if (b > sh.sms * 8) b = sh.sms * 8;
+        mixed_star_kernel<true><<<b, 256, 0, stream>>>(none, no_tile, B, mb);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    mixed_retrace_kernel<true><<<sh.sms * per(sh.per_retrace_b), kMixThreads, 0, stream>>>(none, no_tile, B, mb,
+                                                                                            stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int rb = static_cast<int>((B.n_pixels + 255) / 256);
+    if (rb > sh.sms * 8) rb = sh.sms * 8;
+    if (rb < 1) rb = 1;
+    mixed_resolve_kernel<true><<<rb, 256, 0, stream>>>(none, no_tile, B, mb, out_rgba, nullptr, nullptr, stats);
+    return cudaGetLastError();
 }
 
 }  // namespace grrt_b200

@@ -50,8 +50,9 @@ struct LaunchResources {
 // Doubles of spectral scratch a launch with nb bins needs on the current device.
 size_t volume_spectral_scratch_elems(int nb);
 
+// Thin-disk render, FP64 form.
 cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                        const LaunchResources& res, int form, cudaStream_t stream);
+                        const LaunchResources& res, cudaStream_t stream);
 
 cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                               const LaunchResources& res, int form, cudaStream_t stream);
@@ -90,10 +91,20 @@ cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const D
 cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
                                  const ThinOutputs& out, DevStats* stats, cudaStream_t stream);
 
-// Batched thin-disk render over many cameras (see DevBatch).
-cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,
+// Batched thin-disk render over many cameras (see DevBatch), FP64 form.
+cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats,
                               int blocks, cudaStream_t stream);
-int thin_batch_max_blocks_per_sm(int form);
+int thin_batch_max_blocks_per_sm();
+
+// Batched mixed form: the four phases of launch_thin_mixed, each one launch
+// over the samples of every item (B.n_items, n_samples, n_pixels and each
+// item's sample0 set). Scratch: mixed_scratch_bytes_for(B.n_samples).
+// any_stars: some scene has stars on. blocks_per_sm: 0 = as many as fit.
+size_t mixed_scratch_bytes_for(size_t n_samples);
+cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* out_rgba, unsigned* queue,
+                                    DevStats* stats, void* scratch, size_t scratch_bytes, int blocks_per_sm,
+                                    cudaStream_t stream);
+int mixed_batch_max_blocks_per_sm();
 
 // Spectral render whose scratch is a file-scope device array (no allocation);
 // see vol_render.cu. Returns cudaErrorInvalidValue when nb exceeds the limit.

@@ -80,10 +80,14 @@ struct DevScene {
     int vol_on = 0;
     DevVolume vol;
 
-    // mixed-precision form: outer steps starting at r > fp32_r_min use FP32
-    // right-hand sides, controlled against tol_fp32
+    // mixed-precision forms. Volumetric: outer steps starting at r >
+    // fp32_r_min use FP32 right-hand sides, controlled against tol_fp32.
+    // Thin disk: the FP32 speculation runs against tol_fp32 and re-traces in
+    // FP64 the escapes that came inside fp32_r_min and the samples whose
+    // crossings fall within mixed_margin of a disk edge.
     double fp32_r_min = 0;
     double tol_fp32 = 1e-6;
+    double mixed_margin = 0.05;
 };
 
 // Which pixels a launch covers: the rectangle [x0, x0+w) x [y0, y0+h) of the
@@ -101,6 +105,7 @@ struct DevBatchItem {
     int x0 = 0, y0 = 0, w = 0, h = 0;
     int out_pitch = 0;           // output row pitch in pixels
     size_t out_offset = 0;       // first output pixel of this item
+    size_t sample0 = 0;          // first sample of this item (mixed form: samples of all items in item order)
 };
 struct DevBatchChunk {
     int item = 0;
@@ -113,6 +118,10 @@ struct DevBatch {
     const DevBatchChunk* chunks = nullptr;
     int n_chunks = 0;
     int chunk_size = 1;
+    // mixed form: the items in order (ascending out_offset and sample0)
+    int n_items = 0;
+    unsigned n_samples = 0;      // sum over items of w * h * grid^2
+    size_t n_pixels = 0;         // sum over items of w * h
 };
 
 // Per-launch counters (summed over all threads with one atomic per warp).

@@ -2,7 +2,8 @@
 // emission summed over every equatorial crossing inside [r_in, r_out] ->
 // first-match star lookup on escape. The per-pixel path of
 // GeodesicTracer::trace (src/geodesic_tracer.cpp:23-181) inside the loop of
-// Renderer::render (src/renderer.cpp:30-82), for both precision forms.
+// Renderer::render (src/renderer.cpp:30-82), in the FP64 form (the mixed form
+// of the thin disk is mixed_render.cu).
 //
 // Execution model: a persistent grid (resident blocks only). Each lane owns one
 // pixel at a time and walks its spp samples; each loop iteration performs
@@ -74,7 +75,7 @@ __device__ __forceinline__ int start_check(const DevScene& S, int step, double r
 // kBatch = true: work index -> (chunk, offset) through the batch's chunk table,
 // so one launch covers many cameras (scenes[item.scene]) in the order the
 // schedule lists the chunks.
-template <int kForm, bool kBatch>
+template <bool kBatch>
 __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B, const DevTile& tile,
                                           float4* __restrict__ out_rgba, double* __restrict__ out_rgb64,
                                           uint32_t* __restrict__ out_fate, unsigned total,
@@ -169,19 +170,10 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
         // ---- one DP45 attempt for every lane with a live, unterminated ray ----
         if (live && term < 0) {
             Vec5<double> y5;
-            double err;
-            double tol = S.tol;
-            if (kForm == kFormMixed && y.r > S.fp32_r_min) {
-                Vec5<float> k7;
-                err = mixed_attempt_impl(static_cast<float>(S.M), static_cast<float>(S.a),
-                                         static_cast<float>(pt), static_cast<float>(pph), y, dl, y5, k7);
-                tol = S.tol_fp32;
-            } else {
-                err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
-                ++cnt.fp64_attempts;
-            }
+            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            ++cnt.fp64_attempts;
             ++cnt.attempts;
-            const StepDecision d = pi_control(err, tol, dl, retry, y5.r);
+            const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
             if (d.accept) {
                 ++cnt.accepted;
                 // equatorial crossing (src/geodesic_tracer.cpp:156-176): every
@@ -272,36 +264,33 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
     flush_counters(stats, cnt, cancelled);
 }
 
-template <int kForm>
 __global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
 thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
                    double* __restrict__ out_rgb64, uint32_t* __restrict__ out_fate,
                    unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
                    const volatile int* __restrict__ cancel) {
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
-    thin_loop<kForm, false>(S, DevBatch{}, tile, out_rgba, out_rgb64, out_fate, total, queue, stats, cancel);
+    thin_loop<false>(S, DevBatch{}, tile, out_rgba, out_rgb64, out_fate, total, queue, stats, cancel);
 }
 
 // One launch over many cameras: the batched form. Work index space =
 // n_chunks * chunk_size (short chunks padded).
-template <int kForm>
 __global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
 thin_batch_kernel(const __grid_constant__ DevBatch B, float4* __restrict__ out_rgba, unsigned int* __restrict__ queue,
                   DevStats* __restrict__ stats) {
     const unsigned total = static_cast<unsigned>(B.n_chunks) * static_cast<unsigned>(B.chunk_size);
-    thin_loop<kForm, true>(B.scenes[0], B, DevTile{}, out_rgba, nullptr, nullptr, total, queue, stats, nullptr);
+    thin_loop<true>(B.scenes[0], B, DevTile{}, out_rgba, nullptr, nullptr, total, queue, stats, nullptr);
 }
 
-template <int kForm>
-static cudaError_t launch_thin_form(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                                    const LaunchResources& res, cudaStream_t stream) {
+cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                        const LaunchResources& res, cudaStream_t stream) {
     static int blocks_per_sm = 0;
     static int num_sms = 0;
     if (blocks_per_sm == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, thin_render_kernel<kForm>, kThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, thin_render_kernel, kThreads, 0);
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
@@ -311,35 +300,23 @@ static cudaError_t launch_thin_form(const DevScene& S, const DevTile& tile, cons
     if (needed < blocks) blocks = needed;
     cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    thin_render_kernel<kForm><<<blocks, kThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate,
-                                                               res.queue, res.stats, res.cancel);
+    thin_render_kernel<<<blocks, kThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
+                                                        res.stats, res.cancel);
     return cudaGetLastError();
 }
 
-cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                        const LaunchResources& res, int form, cudaStream_t stream) {
-    if (form == kFormMixed) return launch_thin_form<kFormMixed>(S, tile, out, res, stream);
-    return launch_thin_form<kFormFP64>(S, tile, out, res, stream);
-}
-
-int thin_batch_max_blocks_per_sm(int form) {
+int thin_batch_max_blocks_per_sm() {
     int n = 0;
-    if (form == kFormMixed)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel<kFormMixed>, kThreads, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel<kFormFP64>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel, kThreads, 0);
     return n < 1 ? 1 : n;
 }
 
-cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int form,
-                              int blocks, cudaStream_t stream) {
+cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int blocks,
+                              cudaStream_t stream) {
     if (B.n_chunks <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    if (form == kFormMixed)
-        thin_batch_kernel<kFormMixed><<<blocks, kThreads, 0, stream>>>(B, out_rgba, queue, stats);
-    else
-        thin_batch_kernel<kFormFP64><<<blocks, kThreads, 0, stream>>>(B, out_rgba, queue, stats);
+    thin_batch_kernel<<<blocks, kThreads, 0, stream>>>(B, out_rgba, queue, stats);
     return cudaGetLastError();
 }
 

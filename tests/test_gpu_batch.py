@@ -65,6 +65,58 @@ def test_batch_device_graph_replay_and_autotune(grrt, need_gpu):
             np.testing.assert_array_equal(got[a:b].reshape(w.shape), w)
 
 
+def single_renders_form(grrt, cams, form):
+    out = []
+    for c in cams:
+        R = grrt.Renderer(c)
+        R.set_precision(form)
+        out.append(R.render())
+        R.close()
+    return out
+
+
+def test_batch_mixed_equals_single_mixed_renders(grrt, need_gpu):
+    """Mixed form: the batch runs the mixed pipeline over one sample space of
+    all cameras, so each camera's image equals its own mixed render bit for
+    bit, for any schedule and through the graph replay; and it meets the mixed
+    form's bar against the FP64 render (relative 1e-4)."""
+    import torch
+    cams = small_sweep(grrt)
+    cams[3] = dict(cams[3], samples_per_pixel=4, width=40, height=32)  # uneven sizes and spp
+    cams.append(grrt.config_params(1, width=36, height=44))           # a scene without stars
+    want = single_renders_form(grrt, cams, grrt.FORM_MIXED)
+    f64 = single_renders_form(grrt, cams, grrt.FORM_FP64)
+    B = grrt.Batch(cams)
+    B.set_precision(grrt.FORM_MIXED)
+    for bp in (0, 1):
+        B.set_schedule(256, B.ORDER_ROUND_ROBIN, bp)
+        got = B.render()
+        for k, (g, w) in enumerate(zip(got, want)):
+            np.testing.assert_array_equal(g, w, err_msg=f"camera {k}, blocks/SM {bp}")
+    st = B.stats()
+    n_samples = sum(c["width"] * c["height"] * c.get("samples_per_pixel", 1) for c in cams)
+    assert st["rays"] == n_samples
+    assert st["horizon"] + st["escaped"] + st["max_steps"] == n_samples
+    assert 0 < st["fp64_attempts"] < 0.5 * st["attempts"]
+    for k, (g, f) in enumerate(zip(got, f64)):
+        scale = float(np.max(f[..., :3]))
+        rel = np.abs(g[..., :3] - f[..., :3]) / np.maximum(np.abs(f[..., :3]), 1e-6 * scale)
+        assert float(rel.max()) <= 1e-4, f"camera {k}: {float(rel.max()):.2e} against the FP64 form"
+    total = int(B.offsets[-1])
+    buf = torch.full((total, 4), float("nan"), dtype=torch.float32, device="cuda")
+    for _ in range(2):  # the second call replays the captured graph
+        B.render_device(buf)
+        torch.cuda.synchronize()
+        g = buf.cpu().numpy()
+        for k, w in enumerate(want):
+            a, b = int(B.offsets[k]), int(B.offsets[k + 1])
+            np.testing.assert_array_equal(g[a:b].reshape(w.shape), w)
+    # switching back gives the FP64 images
+    B.set_precision(grrt.FORM_FP64)
+    for g, f in zip(B.render(), f64):
+        np.testing.assert_array_equal(g, f)
+
+
 def test_batch_rejects_volumetric(grrt):
     cams = [grrt.config_params(3, width=16, height=16)]
     with pytest.raises(RuntimeError, match="thin-disk"):
