@@ -78,6 +78,10 @@ def parse():
     # the learned surrogate (trained in this run) on its evaluation frame; 0 skips it
     ap.add_argument("--surrogate-steps", type=int, default=20000)
     ap.add_argument("--surrogate-size", type=int, default=2048)
+    # the volumetric spectral render (both forms) reported beside the headline
+    ap.add_argument("--no-volumetric", action="store_true")
+    ap.add_argument("--volumetric", action="store_true", help="run only the volumetric spectral section")
+    ap.add_argument("--vol-size", type=int, default=512, help="volumetric frame side (profiler captures)")
     return ap.parse_args()
 
 
@@ -369,6 +373,94 @@ def form_error(torch, grrt, params):
             "rel_floor": "max(|fp64|, 1e-6 x frame max)"}
 
 
+# counted FP64 operations of the volumetric spectral path (transcendental
+# calls not counted): an RK4 march step (4 right-hand sides + stage sums), a
+# clamp evaluation (one right-hand side), one bin of a physics step (opacity
+# trilinear in ln kappa, Planck function, transfer update: 56 plus log10 and 3 exp)
+F_RK4 = 4 * F_EVAL + 70
+F_BIN = 56
+
+
+def run_volumetric(args, torch, G, stream, flush, p64):
+    """Volumetric spectral render: Kerr a=0.9, 512x512, 1 spp, Shakura-Sunyaev
+    alpha 0.1, fBm turbulence 0.4, 2 octaves, seed 42, outer radius 20 M,
+    M = 10 M_sun at 0.1 Eddington, 32 log-spaced bins 1e14..1e18 Hz. Both
+    precision forms, through grrt_render_spectral_device on device buffers,
+    CUDA events on the launching stream, L2 flushed between frames."""
+    freqs = G.log_bins(1e14, 1e18, 32)
+    vw = vh = args.vol_size
+    nb = len(freqs)
+    R = G.Renderer(G.config_params(3, width=vw, height=vh), freqs=freqs)
+    spec = torch.empty((vh, vw, nb), dtype=torch.float64, device="cuda")
+    fate = torch.empty((vh * vw,), dtype=torch.int32, device="cuda")
+    out = {}
+    for name, form in (("fp64", G.FORM_FP64), ("mixed", G.FORM_MIXED)):
+        R.set_precision(form)
+        for _ in range(args.warmup):
+            R.render_spectral_device(spec, vw, vh, fate, stream)
+        torch.cuda.synchronize()
+        ts, phases = [], []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                R.render_spectral_device(spec, vw, vh, fate, stream)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            phases.append(R.phase_ms())
+        ms = float(np.mean(ts))
+        st = R.stats()
+        out[name] = {"ms_per_step": ms, "pixel_freq_per_s": vw * vh * nb / (ms * 1e-3),
+                     "rays_per_s": vw * vh / (ms * 1e-3), "phase_ms": [float(x) for x in np.mean(phases, axis=0)],
+                     "stats": {k: st[k] for k in ("attempts", "fp64_attempts", "march_steps", "clamp_evals",
+                                                  "physics_steps", "bin_updates", "rays", "horizon", "escaped")},
+                     "spec": spec.cpu().numpy(), "fate": fate.cpu().numpy()}
+    f, m = out["fp64"], out["mixed"]
+    scale = float(f["spec"].max())
+    rel = np.abs(m["spec"] - f["spec"]) / np.maximum(np.abs(f["spec"]), 1e-6 * scale)
+    flux_f = f["spec"].sum(axis=(0, 1))
+    flux_m = m["spec"].sum(axis=(0, 1))
+    err = {"bit_identical": bool(np.array_equal(m["spec"], f["spec"])), "max_rel": float(rel.max()),
+           "pixels_above_1e-4": int(np.sum(rel.max(axis=2) > 1e-4)),
+           "flux_max_rel_per_bin": float(np.max(np.abs(flux_m - flux_f) / np.maximum(np.abs(flux_f), 1e-300))),
+           "fate_differences": int(np.sum(m["fate"] != f["fate"]))}
+    st = f["stats"]
+    flops = st["attempts"] * F_ATTEMPT + st["march_steps"] * F_RK4 + st["clamp_evals"] * F_EVAL + \
+        st["bin_updates"] * F_BIN
+    kms = f["phase_ms"][0]
+    ach = flops / (kms * 1e-3) / 1e12
+    cube = vw * vh * nb * 8
+    res = {"config": {"workload": f"volumetric_kerr_a0.9_{vw}x{vh}_1spp_32bins_1e14-1e18Hz_alpha0.1_turb0.4_oct2",
+                      "bins": nb, "width": vw, "height": vh, "l2": "flushed between steps (256 MiB write)"},
+           "metric": "pixel*frequency/s", "value": m["pixel_freq_per_s"], "headline_form": "mixed",
+           "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("spec", "fate")} for k, v in out.items()},
+           "speedup_mixed_vs_fp64": f["ms_per_step"] / m["ms_per_step"], "mixed_error_vs_fp64": err,
+           "roofline_fp64": {"kernel": "vol_spectral_kernel<false>", "bound": "fp64", "achieved": ach, "peak": p64,
+                             "unit": "TFLOP/s", "frac": ach / p64,
+                             "flop_count": f"{F_ATTEMPT}/attempt, {F_RK4}/march step, {F_EVAL}/clamp, "
+                                           f"{F_BIN}/bin update (transcendentals not counted), device counters"},
+           "cube_store": {"bytes": cube, "GB_per_s": cube / (kms * 1e-3) / 1e9}}
+    if not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import oracle_bind
+            kind = "fast" if oracle_bind.ref_available("fast") else "strict"
+            ref = oracle_bind.RefScene(G.config_params(3, width=vw, height=vh), freqs=freqs, kind=kind)
+            stride = 8
+            _, secs, threads = ref.render_spectral_rows(0, stride)
+            npf = len(range(0, vh, stride)) * vw * nb
+            res["cpu_baseline"] = {"value": npf / secs, "unit": "pixel*frequency/s", "cores": threads,
+                                   "kind": "reference",
+                                   "sample": f"rows 0,{stride},...,{vh - stride} of the frame, reference src/*.cpp "
+                                             f"({kind} build) via oracle/_ref, OpenMP, {secs:.2f} s"}
+        except Exception as ex:
+            res["cpu_baseline"] = {"value": None, "sample": f"unavailable: {ex}"}
+    R.close()
+    return res
+
+
 def sgemm_peak(torch) -> float:
     """FP32 (non-tensor) roofline denominator: cuBLAS SGEMM 8192^3 with TF32 off, best of 5."""
     prev = torch.backends.cuda.matmul.allow_tf32
@@ -500,6 +592,23 @@ def main():
     args = parse()
     if args.batch:
         run_batch(args)
+        return
+    if args.volumetric:
+        # the volumetric spectral render alone (one GPU), as its own JSON line
+        import torch
+        import grrt_b200 as G
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        stream = torch.cuda.Stream()
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        p64 = measured_peaks(torch)["fp64_tflops_dgemm"]
+        clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clocks.start()
+        res = run_volumetric(args, torch, G, stream, flush, p64)
+        res["clocks"] = clocks.stop()
+        res.update(n_gpus=1, steps=args.steps, warmup=args.warmup, unit="pixel*frequency/s",
+                   higher_is_better=True, data="synthetic", dtype="f32+f64",
+                   gpu_launches=args.steps * 3)
+        print(json.dumps(res), flush=True)
         return
     if (args.width, args.height) != (W, H):
         W, H = args.width, args.height
@@ -634,6 +743,11 @@ def main():
                          "crossings": head["stats"]["crossings"],
                          "fp64_attempt_share": head["stats"]["fp64_attempts"] / max(1, head["stats"]["attempts"])},
                 "kernel_ms_per_step": head["kernel_ms"], "wall_s_timed_region": head["wall"]}
+        if not args.no_volumetric:
+            try:
+                line["volumetric"] = run_volumetric(args, torch, G, stream, flush, p64)
+            except Exception as ex:  # reported, the headline stands on its own
+                line["volumetric"] = {"error": str(ex)}
         if args.surrogate_steps > 0:
             try:
                 line["surrogate"] = run_surrogate(args, torch, G, stream, flush, peaks)

@@ -119,6 +119,12 @@ void GRRTContext::build(const GRRTParams& p) {
                 ln_kabs[i] = std::log(std::max(vol->opacity.kappa_abs[i], 1e-100));
             std::printf("[GRRT] volumetric disk: r_isco=%.4f r_horizon=%.4f rho_scale=%.4e\n", vol->r_isco,
                         vol->r_horizon, vol->rho_scale);
+            // half-thickness of the near-disk clamp slab, z_max + 6 H, at its
+            // widest (the radial tables are linear between nodes and constant
+            // beyond them)
+            vol_reach_z = 0.0;
+            for (size_t i = 0; i < vol->H.size() && i < vol->z_max.size(); ++i)
+                vol_reach_z = std::max(vol_reach_z, vol->z_max[i] + 6.0 * vol->H[i]);
         }
     }
     has_stars = p.background_type == GRRT_BG_STARS;
@@ -335,7 +341,7 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
         }
     }
     n_phases = 0;
-        cudaEventRecord(ev0, s);
+    cudaEventRecord(ev0, s);
     cudaError_t e;
     if (vol)
         e = launch_volume_rgb(S, tile, out, res, form, s);
@@ -458,10 +464,25 @@ int GRRTContext::render_spectral_device(int width, int height, double* d_spec, u
     out.spec = d_spec;
     out.fate = d_fate;
     const DevScene S = scene_for_launch();
+    const bool mixed = form == GRRT_FORM_MIXED;
+    if (mixed) {
+        const size_t mb = volume_mixed_scratch_bytes(tile, S.grid * S.grid, nb);
+        if (mb > d_mixed_scratch_bytes) {
+            cudaFree(d_mixed_scratch);
+            d_mixed_scratch = nullptr;
+            d_mixed_scratch_bytes = 0;
+            if (fail_cuda(cudaMalloc(&d_mixed_scratch, mb), "cudaMalloc(mixed scratch)")) return -1;
+            d_mixed_scratch_bytes = mb;
+        }
+    }
     n_phases = 0;
-        cudaEventRecord(ev0, s);
-    cudaError_t e = launch_volume_spectral(S, tile, d_freqs, nb, out, res, form, s);
+    cudaEventRecord(ev0, s);
+    const cudaError_t e =
+        mixed ? launch_volume_spectral_mixed(S, tile, d_freqs, nb, out, res, d_mixed_scratch, d_mixed_scratch_bytes,
+                                             vol_reach_z, ev_phase, s)
+              : launch_volume_spectral(S, tile, d_freqs, nb, out, res, s);
     cudaEventRecord(ev1, s);
+    n_phases = mixed ? kVolMixedPhases : 0;
     return fail_cuda(e, "spectral launch") ? -1 : 0;
 }
 

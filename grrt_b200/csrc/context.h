@@ -37,6 +37,7 @@ struct GRRTContext {
     double mixed_r_factor = 3.0;
     double tol_fp32 = 1e-6;
     double mixed_margin = 0.05;  // disk-radius margin (M) of the mixed form's re-trace test
+    double vol_reach_z = 0.0;    // volumetric: max over r of z_max + 6 H (the mixed form's speculation bound)
 
     std::string error;
     float progress = 0.0f;
@@ -52,8 +53,9 @@ struct GRRTContext {
     int* d_cancel = nullptr;   // its device alias
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // per-kernel phases of the last render (mixed form: speculate, stars,
-    // re-trace, resolve; otherwise the one render kernel)
+    // per-kernel phases of the last render (thin mixed form: speculate, stars,
+    // re-trace, resolve; volumetric spectral mixed form: speculate, re-trace,
+    // resolve; otherwise the one render kernel)
     cudaEvent_t ev_phase[grrt_b200::kMixedPhases + 1] = {};
     int n_phases = 0;
     double last_kernel_ms = 0.0;

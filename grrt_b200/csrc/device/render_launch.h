@@ -57,9 +57,26 @@ cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutput
 cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                               const LaunchResources& res, int form, cudaStream_t stream);
 
+// Spectral render, FP64 form (vol_spectral.cu: warp-cooperative transfer).
+constexpr int kVolSpectralThreads = 128;
 cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
-                                   const SpectralOutputs& out, const LaunchResources& res, int form,
-                                   cudaStream_t stream);
+                                   const SpectralOutputs& out, const LaunchResources& res, cudaStream_t stream);
+// The same kernel on a caller-chosen grid of kVolSpectralThreads-thread blocks
+// and scratch (4 * nb doubles per thread); *queue must be zero.
+cudaError_t launch_vol_spectral_on(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
+                                   double* out_spec, uint32_t* out_fate, double* scratch, unsigned* queue,
+                                   DevStats* stats, const volatile int* cancel, int blocks, cudaStream_t stream);
+// Mixed form of the spectral render: FP32 speculation, FP64 re-trace of the
+// samples that may reach the volume, resolve. reach_z = max over the radial
+// tables of z_max + 6 H. Scratch: volume_mixed_scratch_bytes; res must hold
+// the spectral scratch as for launch_volume_spectral. phase_events: NULL or
+// kVolMixedPhases + 1 events (speculate, re-trace, resolve).
+constexpr int kVolMixedPhases = 3;
+size_t volume_mixed_scratch_bytes(const DevTile& tile, int g2, int nb);
+cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
+                                         const SpectralOutputs& out, const LaunchResources& res, void* scratch,
+                                         size_t scratch_bytes, double reach_z, cudaEvent_t* phase_events,
+                                         cudaStream_t stream);
 
 // Mixed-precision thin-disk render: FP32 speculation, FP64 re-trace, resolve.
 size_t mixed_scratch_bytes(const DevTile& tile, int g2);

@@ -1,14 +1,14 @@
-// Volumetric disk renders, RGB and spectral: the outer adaptive DP45 loop with
-// the near-disk step clamp and the ray-march hand-over
-// (src/geodesic_tracer.cpp:23-181 and 495-603), and the fixed-step RK4 march
-// with per-channel or per-bin radiative transfer
-// (src/geodesic_tracer.cpp:183-337 and 605-746).
+// Volumetric disk, RGB render: the outer adaptive DP45 loop with the
+// near-disk step clamp and the ray-march hand-over
+// (src/geodesic_tracer.cpp:23-181), and the fixed-step RK4 march with
+// three-channel radiative transfer (src/geodesic_tracer.cpp:183-337). The
+// spectral render is vol_spectral.cu; the spectral entry point without device
+// allocation (below) launches that kernel on a fixed scratch.
 //
 // Same persistent execution model as the thin-disk kernel: a lane owns one
 // pixel, one loop iteration advances each live ray by one DP45 attempt (outer
-// phase) or one RK4 march step (march phase). Spectral transfer state
-// (J, T, tau and the pixel sum, per bin) sits in a global scratch laid out
-// [array][bin][lane slot], so the 32 lanes of a warp touch consecutive words.
+// phase) or one RK4 march step (march phase); the three channels' transfer
+// state sits in registers. Both precision forms run the FP64 method here.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -17,6 +17,7 @@
 #include "integrate.cuh"
 #include "render_launch.h"
 #include "shading.cuh"
+#include "vol_steps.cuh"
 #include "volume.cuh"
 
 namespace grrt_b200 {
@@ -26,34 +27,6 @@ namespace {
 constexpr int kVolThreads = 128;
 constexpr unsigned kFullMask = 0xffffffffu;
 
-struct VolCounters {
-    unsigned long long attempts = 0, accepted = 0, rays = 0, horizon = 0, escaped = 0, maxsteps = 0;
-    unsigned long long clamp = 0, march = 0, physics = 0, bins = 0, fp64 = 0;
-};
-
-__device__ __forceinline__ void flush_vol(DevStats* st, const VolCounters& c, bool cancelled) {
-    unsigned long long v[11] = {c.attempts, c.accepted, c.rays, c.horizon, c.escaped, c.maxsteps,
-                                c.clamp, c.march, c.physics, c.bins, c.fp64};
-#pragma unroll
-    for (int k = 0; k < 11; ++k)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(kFullMask, v[k], o);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&st->attempts, v[0]);
-        atomicAdd(&st->accepted, v[1]);
-        atomicAdd(&st->rays, v[2]);
-        atomicAdd(&st->horizon, v[3]);
-        atomicAdd(&st->escaped, v[4]);
-        atomicAdd(&st->max_steps, v[5]);
-        atomicAdd(&st->clamp_evals, v[6]);
-        atomicAdd(&st->march_steps, v[7]);
-        atomicAdd(&st->physics_steps, v[8]);
-        atomicAdd(&st->bin_updates, v[9]);
-        atomicAdd(&st->fp64_attempts, v[10]);
-        if (cancelled && threadIdx.x == 0) atomicAdd(&st->cancelled, 1ull);
-    }
-}
-
 // Observer-frame RGB frequencies (450, 550, 650 nm) of the RGB transfer.
 __device__ __forceinline__ double rgb_nu(int ch) {
     constexpr double c = 2.997924e10;
@@ -62,24 +35,16 @@ __device__ __forceinline__ double rgb_nu(int ch) {
 
 }  // namespace
 
-// kSpectral = false: three channels in registers, opaque when all T < 1e-6.
-// kSpectral = true: nb bins in scratch, optically thick when all tau > 10.
-template <bool kSpectral, int kForm>
+// Three channels in registers; the march ends when all T < 1e-6.
 __global__ void __launch_bounds__(kVolThreads)
-vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const double* __restrict__ freqs,
-                  int nb, float4* __restrict__ out_rgba, double* __restrict__ out_d, uint32_t* __restrict__ out_fate,
-                  double* __restrict__ scratch, unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
-                  const volatile int* __restrict__ cancel) {
+vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
+                  double* __restrict__ out_d, uint32_t* __restrict__ out_fate, unsigned int* __restrict__ queue,
+                  DevStats* __restrict__ stats, const volatile int* __restrict__ cancel) {
     const DevVolume& V = S.vol;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
     const int grid2 = S.grid * S.grid;
-    const size_t slot = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    const size_t nslot = static_cast<size_t>(gridDim.x) * blockDim.x;
-    // spectral scratch: J, T, tau, pixel sum; element (array, bin) at [(array*nb + bin)*nslot + slot]
-    auto sc = [&](int arr, int b) -> double& { return scratch[(static_cast<size_t>(arr) * nb + b) * nslot + slot]; };
-    const int med = nb / 2;
 
     VolCounters cnt;
     int pix = -1, smp = 0;
@@ -90,7 +55,6 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
     int retry = 0, step = 0, entries = 0;
     // transfer state (RGB in registers)
     double J[3] = {0.0, 0.0, 0.0}, Tt[3] = {1.0, 1.0, 1.0};
-    int n_thick = 0;
     // march state
     Vec5<double> ms{};
     double ds = 0.0;
@@ -114,8 +78,6 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
                     pix = static_cast<int>(q);
                     smp = 0;
                     acc[0] = acc[1] = acc[2] = 0.0;
-                    if (kSpectral)
-                        for (int b = 0; b < nb; ++b) sc(3, b) = 0.0;
                 } else {
                     pix = -2;
                 }
@@ -138,13 +100,6 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
             marching = false;
             J[0] = J[1] = J[2] = 0.0;
             Tt[0] = Tt[1] = Tt[2] = 1.0;
-            n_thick = 0;
-            if (kSpectral)
-                for (int b = 0; b < nb; ++b) {
-                    sc(0, b) = 0.0;
-                    sc(1, b) = 1.0;
-                    sc(2, b) = 0.0;
-                }
             live = true;
             need_start = true;
         }
@@ -156,23 +111,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
             else if (y.r < S.r_stop) term = kTermHorizon;
             else if (y.r > S.r_escape) term = kTermEscaped;
             if (term < 0) {
-                const double r = y.r;
-                if (r >= V.r_horizon * 0.9 && r <= V.r_outer * 1.5) {
-                    double st, ct;
-                    sincos(y.th, &st, &ct);
-                    const double z = r * ct;
-                    const double H = v_scale_height(V, r);
-                    const double zm = v_zmax(V, r);
-                    if (fabs(z) < zm + 6.0 * H) {
-                        const Vec5<double> d = kerr_rhs<double>(S.M, S.a, pt, pph, y);
-                        ++cnt.clamp;
-                        const double dz_dl = fabs(ct * d.r - r * st * d.th);
-                        if (dz_dl > 1e-20) {
-                            const double dl_max = vmax(0.25 * H / dz_dl, H / 64.0);
-                            dlambda = vmin(dlambda, dl_max);
-                        }
-                    }
-                }
+                if (vol_clamp(S, pt, pph, y, dlambda)) ++cnt.clamp;
                 prev = y;
                 dl = dlambda;
                 retry = 0;
@@ -183,18 +122,10 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
         if (live && term < 0 && !marching) {
             // ---- one DP45 attempt ----
             Vec5<double> y5;
-            double err, tol = S.tol;
-            if (kForm == kFormMixed && y.r > S.fp32_r_min) {
-                Vec5<float> k7;
-                err = mixed_attempt_impl(static_cast<float>(S.M), static_cast<float>(S.a), static_cast<float>(pt),
-                                         static_cast<float>(pph), y, dl, y5, k7);
-                tol = S.tol_fp32;
-            } else {
-                err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
-                ++cnt.fp64;
-            }
+            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            ++cnt.fp64;
             ++cnt.attempts;
-            const StepDecision d = pi_control(err, tol, dl, retry, y5.r);
+            const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
             if (!d.accept) {
                 dl = d.next;
                 ++retry;
@@ -204,37 +135,14 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
                 dlambda = d.next;
                 ++step;  // the reference's loop counter advances on every outer iteration
                 // hand-over to the ray-march (src/geodesic_tracer.cpp:105-153)
-                bool opaque = false;
-                if (!kSpectral) opaque = (Tt[0] < 1e-6 && Tt[1] < 1e-6 && Tt[2] < 1e-6);
-                if (!opaque) {
-                    const double hp = kHalfPi;
-                    const double d_prev = prev.th - hp, d_new = y.th - hp;
-                    const double r_new = y.r, r_prev = prev.r;
-                    const double z_new = r_new * cos(y.th);
-                    const double z_prev = r_prev * cos(prev.th);
-                    const bool crossed = (d_prev * d_new < 0.0) && fabs(d_prev - d_new) > 1e-12;
-                    const bool inside_now = v_inside(V, r_new, z_new);
-                    const double zm_new = v_zmax(V, r_new), H_new = v_scale_height(V, r_new);
-                    const double H_prev = v_scale_height(V, r_prev);
-                    const bool near = (fabs(z_new) < zm_new + 2.0 * H_new ||
-                                       fabs(z_prev) < v_zmax(V, r_prev) + 2.0 * H_prev) &&
-                                      r_new >= V.r_horizon && r_new <= V.r_outer;
-                    if (crossed || inside_now || near) {
-                        const double r_lo = vmin(r_prev, r_new), r_hi = vmax(r_prev, r_new);
-                        if (r_hi >= V.r_horizon && r_lo <= V.r_outer && r_prev >= V.r_horizon * 0.9 &&
-                            r_prev <= V.r_outer * 1.5) {
-                            // march from the pre-step state
-                            marching = true;
-                            ++entries;
-                            ms = prev;
-                            const double r0 = ms.r;
-                            const double z0 = r0 * cos(ms.th);
-                            const double H0 = v_scale_height(V, r0);
-                            been_inside = v_inside(V, r0, z0);
-                            ds = been_inside ? H0 / 16.0 : vmin(fabs(z0) / 8.0, H0 * 2.0);
-                            mcount = 0;
-                        }
-                    }
+                const bool opaque = (Tt[0] < 1e-6 && Tt[1] < 1e-6 && Tt[2] < 1e-6);
+                if (!opaque && vol_enters(V, prev, y)) {
+                    // march from the pre-step state
+                    marching = true;
+                    ++entries;
+                    ms = prev;
+                    ds = vol_march_start(V, ms, been_inside);
+                    mcount = 0;
                 }
                 // the next outer step starts now, or when the march ends
                 if (!marching) need_start = true;
@@ -251,7 +159,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
             bool end = false;
             if (r < V.r_horizon || r > V.r_outer) {
                 end = true;
-            } else if (kSpectral ? (n_thick == nb) : (Tt[0] < 1e-6 && Tt[1] < 1e-6 && Tt[2] < 1e-6)) {
+            } else if (Tt[0] < 1e-6 && Tt[1] < 1e-6 && Tt[2] < 1e-6) {
                 end = true;
             } else {
                 const double H = v_scale_height(V, r);
@@ -280,31 +188,20 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
                         const double ke = v_kappa_es(V, ir, fr, iT, fT);
                         const double ag = fabs(g);
                         double ka_med = 0.0;
-                        const int nbins = kSpectral ? nb : 3;
-                        for (int b = 0; b < nbins; ++b) {
-                            const double nu = ag * (kSpectral ? __ldg(freqs + b) : rgb_nu(b));
+                        for (int b = 0; b < 3; ++b) {
+                            const double nu = ag * rgb_nu(b);
                             const double ka = v_kappa_abs(V, nu, ir, fr, iT, fT);
-                            if (b == (kSpectral ? med : 1)) ka_med = ka;
+                            if (b == 1) ka_med = ka;
                             const double kt = ka + ke;
                             const double eps = (kt > 0.0) ? ka / kt : 1.0;
                             const double dtau = kt * rho * dsp;
                             const double B = planck_nu(nu, Tl);
                             const double Sv = eps * B / (nu * nu * nu);
                             const double e = exp(-dtau);
-                            if (kSpectral) {
-                                double& tau = sc(2, b);
-                                const bool was = !(tau <= 10.0);
-                                tau += dtau;
-                                n_thick += (!(tau <= 10.0)) - was;
-                                double& Tb = sc(1, b);
-                                sc(0, b) += Tb * Sv * (1.0 - e);
-                                Tb *= e;
-                            } else {
-                                J[b] += Tt[b] * Sv * (1.0 - e);
-                                Tt[b] *= e;
-                            }
+                            J[b] += Tt[b] * Sv * (1.0 - e);
+                            Tt[b] *= e;
                         }
-                        cnt.bins += static_cast<unsigned long long>(nbins);
+                        cnt.bins += 3;
                         const double at = (ka_med + ke) * rho;
                         const double ds_tau = (at > 0.0) ? 0.05 / at : ds * 2.0;
                         const double ds_geo = 0.1 * vmax(r - V.r_horizon, 0.5);
@@ -328,23 +225,16 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
             if (term == kTermEscaped) ++cnt.escaped;
             else if (term == kTermHorizon) ++cnt.horizon;
             else ++cnt.maxsteps;
-            if (kSpectral) {
-                for (int b = 0; b < nb; ++b) {
-                    const double f = __ldg(freqs + b);
-                    sc(3, b) += sc(0, b) * f * f * f;
-                }
-            } else {
-                double col[3];
-                for (int ch = 0; ch < 3; ++ch) {
-                    const double nu = rgb_nu(ch);
-                    col[ch] = 0.0 + J[ch] * nu * nu * nu;
-                }
-                if (term == kTermEscaped && S.stars_on) {
-                    const double bright = star_brightness(S.stars, y.th, y.ph);
-                    for (int ch = 0; ch < 3; ++ch) col[ch] += bright;
-                }
-                for (int ch = 0; ch < 3; ++ch) acc[ch] = acc[ch] + col[ch];
+            double col[3];
+            for (int ch = 0; ch < 3; ++ch) {
+                const double nu = rgb_nu(ch);
+                col[ch] = 0.0 + J[ch] * nu * nu * nu;
             }
+            if (term == kTermEscaped && S.stars_on) {
+                const double bright = star_brightness(S.stars, y.th, y.ph);
+                for (int ch = 0; ch < 3; ++ch) col[ch] += bright;
+            }
+            for (int ch = 0; ch < 3; ++ch) acc[ch] = acc[ch] + col[ch];
             if (out_fate) {
                 const unsigned ne = (entries > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(entries);
                 out_fate[static_cast<size_t>(pix) * grid2 + smp] = static_cast<unsigned>(term) | (ne << 2);
@@ -352,19 +242,14 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
             if (++smp == grid2) {
                 const int qx = pix % tile.w, qy = pix / tile.w;
                 const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
-                if (kSpectral) {
-                    double* dst = out_d + o * nb;
-                    for (int b = 0; b < nb; ++b) dst[b] = sc(3, b) * S.inv_spp;
-                } else {
-                    const double r0 = acc[0] * S.inv_spp, r1 = acc[1] * S.inv_spp, r2 = acc[2] * S.inv_spp;
-                    if (out_rgba)
-                        out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1),
-                                                  static_cast<float>(r2), 1.0f);
-                    if (out_d) {
-                        out_d[3 * o + 0] = r0;
-                        out_d[3 * o + 1] = r1;
-                        out_d[3 * o + 2] = r2;
-                    }
+                const double r0 = acc[0] * S.inv_spp, r1 = acc[1] * S.inv_spp, r2 = acc[2] * S.inv_spp;
+                if (out_rgba)
+                    out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1), static_cast<float>(r2),
+                                              1.0f);
+                if (out_d) {
+                    out_d[3 * o + 0] = r0;
+                    out_d[3 * o + 1] = r1;
+                    out_d[3 * o + 2] = r2;
                 }
                 pix = -1;
             }
@@ -384,18 +269,15 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, const 
     flush_vol(stats, cnt, cancelled);
 }
 
-namespace {
-
-template <bool kSpectral, int kForm>
-cudaError_t launch_vol(const DevScene& S, const DevTile& tile, const double* freqs, int nb, float4* rgba,
-                       double* out_d, uint32_t* fate, const LaunchResources& res, cudaStream_t stream) {
+cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                              const LaunchResources& res, int form, cudaStream_t stream) {
+    (void)form;  // the FP64 method serves both forms (see the file comment)
     static int blocks_per_sm = 0, num_sms = 0;
     if (blocks_per_sm == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, vol_render_kernel<kSpectral, kForm>,
-                                                      kVolThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, vol_render_kernel, kVolThreads, 0);
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
@@ -403,47 +285,11 @@ cudaError_t launch_vol(const DevScene& S, const DevTile& tile, const double* fre
     int blocks = num_sms * blocks_per_sm;
     const int needed = static_cast<int>((total + kVolThreads - 1) / kVolThreads);
     if (needed < blocks) blocks = needed;
-    double* scratch = nullptr;
-    if (kSpectral) {
-        // J, T, tau and the pixel sum per bin and lane slot.
-        const size_t need = static_cast<size_t>(4) * nb * blocks * kVolThreads;
-        scratch = res.spectral_scratch;
-        if (!scratch || res.spectral_scratch_elems < need) return cudaErrorInvalidValue;
-    }
     cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    vol_render_kernel<kSpectral, kForm><<<blocks, kVolThreads, 0, stream>>>(
-        S, tile, freqs, nb, rgba, out_d, fate, scratch, res.queue, res.stats, res.cancel);
+    vol_render_kernel<<<blocks, kVolThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
+                                                          res.stats, res.cancel);
     return cudaGetLastError();
-}
-
-}  // namespace
-
-size_t volume_spectral_scratch_elems(int nb) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vol_render_kernel<true, kFormFP64>, kVolThreads, 0);
-    int per_sm_m = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_m, vol_render_kernel<true, kFormMixed>, kVolThreads, 0);
-    if (per_sm_m > per_sm) per_sm = per_sm_m;
-    if (per_sm < 1) per_sm = 1;
-    return static_cast<size_t>(4) * nb * sms * per_sm * kVolThreads;
-}
-
-cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                              const LaunchResources& res, int form, cudaStream_t stream) {
-    if (form == kFormMixed)
-        return launch_vol<false, kFormMixed>(S, tile, nullptr, 0, out.rgba, out.rgb64, out.fate, res, stream);
-    return launch_vol<false, kFormFP64>(S, tile, nullptr, 0, out.rgba, out.rgb64, out.fate, res, stream);
-}
-
-cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
-                                   const SpectralOutputs& out, const LaunchResources& res, int form,
-                                   cudaStream_t stream) {
-    if (form == kFormMixed)
-        return launch_vol<true, kFormMixed>(S, tile, freqs, nb, nullptr, out.spec, out.fate, res, stream);
-    return launch_vol<true, kFormFP64>(S, tile, freqs, nb, nullptr, out.spec, out.fate, res, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -468,7 +314,7 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
 namespace {
 constexpr int kNoAllocMaxBins = 32;
 constexpr int kNoAllocBlocks = 148;  // one block per B200 SM
-constexpr size_t kNoAllocSlots = static_cast<size_t>(kNoAllocBlocks) * kVolThreads;
+constexpr size_t kNoAllocSlots = static_cast<size_t>(kNoAllocBlocks) * kVolSpectralThreads;
 constexpr size_t kNoAllocHeader = 512;  // [0,256): work counter, [256,512): DevStats
 constexpr size_t kNoAllocBytes = kNoAllocHeader + sizeof(double) * 4 * kNoAllocMaxBins * kNoAllocSlots;
 static_assert(sizeof(DevStats) <= 256, "stats must fit the header");
@@ -511,13 +357,11 @@ cudaError_t launch_volume_spectral_noalloc(const DevScene& S, const DevTile& til
     auto* queue = reinterpret_cast<unsigned int*>(base);
     auto* stats = reinterpret_cast<DevStats*>(base + 256);
     auto* transfer = reinterpret_cast<double*>(base + kNoAllocHeader);
-    if (form == kFormMixed)
-        vol_render_kernel<true, kFormMixed><<<kNoAllocBlocks, kVolThreads, 0, stream>>>(
-            S, tile, freqs, nb, nullptr, out_spec, nullptr, transfer, queue, stats, nullptr);
-    else
-        vol_render_kernel<true, kFormFP64><<<kNoAllocBlocks, kVolThreads, 0, stream>>>(
-            S, tile, freqs, nb, nullptr, out_spec, nullptr, transfer, queue, stats, nullptr);
-    return cudaGetLastError();
+    // Both forms: the FP64 kernel. The mixed form's output is bit-identical to
+    // it, and its per-sample buffers would need an allocation.
+    (void)form;
+    return launch_vol_spectral_on(S, tile, freqs, nb, out_spec, nullptr, transfer, queue, stats, nullptr,
+                                  kNoAllocBlocks, stream);
 }
 
 }  // namespace grrt_b200

@@ -1,0 +1,104 @@
+// Pieces of the volumetric trace shared by the volumetric kernels: the
+// near-disk clamp at the start of an outer step, the hand-over test from the
+// outer DP45 loop to the ray-march, the march's starting step, and the
+// per-launch counters (src/geodesic_tracer.cpp:71-153 and 495-603).
+#pragma once
+
+#include "integrate.cuh"
+#include "volume.cuh"
+
+namespace grrt_b200 {
+
+struct VolCounters {
+    unsigned long long attempts = 0, accepted = 0, rays = 0, horizon = 0, escaped = 0, maxsteps = 0;
+    unsigned long long clamp = 0, march = 0, physics = 0, bins = 0, fp64 = 0;
+};
+
+// Warp sum of the counters, one atomic per counter per warp.
+__device__ __forceinline__ void flush_vol(DevStats* st, const VolCounters& c, bool cancelled) {
+    unsigned long long v[11] = {c.attempts, c.accepted, c.rays, c.horizon, c.escaped, c.maxsteps,
+                                c.clamp, c.march, c.physics, c.bins, c.fp64};
+#pragma unroll
+    for (int k = 0; k < 11; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&st->attempts, v[0]);
+        atomicAdd(&st->accepted, v[1]);
+        atomicAdd(&st->rays, v[2]);
+        atomicAdd(&st->horizon, v[3]);
+        atomicAdd(&st->escaped, v[4]);
+        atomicAdd(&st->max_steps, v[5]);
+        atomicAdd(&st->clamp_evals, v[6]);
+        atomicAdd(&st->march_steps, v[7]);
+        atomicAdd(&st->physics_steps, v[8]);
+        atomicAdd(&st->bin_updates, v[9]);
+        atomicAdd(&st->fp64_attempts, v[10]);
+        if (cancelled && threadIdx.x == 0) atomicAdd(&st->cancelled, 1ull);
+    }
+}
+
+// Pixel sum += J nu^3 (I_obs = J nu^3, src/geodesic_tracer.cpp:598-600), each
+// operation rounded on its own (no contraction into a fused multiply-add), so
+// every spectral kernel and the mixed form's resolve produce the same bits.
+__device__ __forceinline__ double add_intensity(double sum, double J, double f) {
+    return __dadd_rn(sum, __dmul_rn(__dmul_rn(__dmul_rn(J, f), f), f));
+}
+
+// Near-disk clamp at the start of an outer step (src/geodesic_tracer.cpp:71-95):
+// for r in [0.9 r_h, 1.5 r_outer] and |z| < z_max + 6 H, dlambda is capped at
+// max(H / (4 |dz/dlambda|), H / 64). Returns whether it evaluated the
+// right-hand side (the clamp counter).
+__device__ __forceinline__ bool vol_clamp(const DevScene& S, double pt, double pph, const Vec5<double>& y,
+                                          double& dlambda) {
+    const DevVolume& V = S.vol;
+    const double r = y.r;
+    if (!(r >= V.r_horizon * 0.9 && r <= V.r_outer * 1.5)) return false;
+    double st, ct;
+    sincos(y.th, &st, &ct);
+    const double z = r * ct;
+    const double H = v_scale_height(V, r);
+    const double zm = v_zmax(V, r);
+    if (!(fabs(z) < zm + 6.0 * H)) return false;
+    const Vec5<double> d = kerr_rhs<double>(S.M, S.a, pt, pph, y);
+    const double dz_dl = fabs(ct * d.r - r * st * d.th);
+    if (dz_dl > 1e-20) {
+        const double dl_max = vmax(0.25 * H / dz_dl, H / 64.0);
+        dlambda = vmin(dlambda, dl_max);
+    }
+    return true;
+}
+
+// Hand-over after an accepted outer step prev -> y (src/geodesic_tracer.cpp:105-153):
+// the step crossed the equator, ends inside the volume, or either end is
+// within z_max + 2H of the plane over the disk's radii; and the step's radii
+// reach [r_h, r_outer] from a start inside [0.9 r_h, 1.5 r_outer]. The march
+// then starts from prev.
+__device__ __forceinline__ bool vol_enters(const DevVolume& V, const Vec5<double>& prev, const Vec5<double>& y) {
+    const double hp = kHalfPi;
+    const double d_prev = prev.th - hp, d_new = y.th - hp;
+    const double r_new = y.r, r_prev = prev.r;
+    const double z_new = r_new * cos(y.th);
+    const double z_prev = r_prev * cos(prev.th);
+    const bool crossed = (d_prev * d_new < 0.0) && fabs(d_prev - d_new) > 1e-12;
+    const bool inside_now = v_inside(V, r_new, z_new);
+    const double zm_new = v_zmax(V, r_new), H_new = v_scale_height(V, r_new);
+    const double H_prev = v_scale_height(V, r_prev);
+    const bool near = (fabs(z_new) < zm_new + 2.0 * H_new || fabs(z_prev) < v_zmax(V, r_prev) + 2.0 * H_prev) &&
+                      r_new >= V.r_horizon && r_new <= V.r_outer;
+    if (!(crossed || inside_now || near)) return false;
+    const double r_lo = vmin(r_prev, r_new), r_hi = vmax(r_prev, r_new);
+    return r_hi >= V.r_horizon && r_lo <= V.r_outer && r_prev >= V.r_horizon * 0.9 && r_prev <= V.r_outer * 1.5;
+}
+
+// First march step length from the start state s: H/16 inside the volume,
+// else min(|z|/8, 2H).
+__device__ __forceinline__ double vol_march_start(const DevVolume& V, const Vec5<double>& s, bool& been_inside) {
+    const double r0 = s.r;
+    const double z0 = r0 * cos(s.th);
+    const double H0 = v_scale_height(V, r0);
+    been_inside = v_inside(V, r0, z0);
+    return been_inside ? H0 / 16.0 : vmin(fabs(z0) / 8.0, H0 * 2.0);
+}
+
+}  // namespace grrt_b200
