@@ -57,8 +57,12 @@ RAYS = W * H * SPP
 #   one DP45 attempt (include/grrt/geodesic/rk4.h:73-177): 7 right-hand sides
 #   + 480 for the stage sums, the 5th-order solution and the error norm over
 #   the reference's 8-component state
+# The kernels take an attempt's first right-hand side from the previous
+# attempt (the same value), so they execute 6 per attempt plus one per ray
+# start; the rooflines count what is executed (F_ATTEMPT_EXEC per attempt +
+# F_EVAL per ray).
 F_EVAL = 133 + 37
-F_ATTEMPT = 7 * F_EVAL + 480
+F_ATTEMPT_EXEC = 6 * F_EVAL + 480
 
 
 def parse():
@@ -427,7 +431,8 @@ def run_volumetric(args, torch, G, stream, flush, p64):
            "flux_max_rel_per_bin": float(np.max(np.abs(flux_m - flux_f) / np.maximum(np.abs(flux_f), 1e-300))),
            "fate_differences": int(np.sum(m["fate"] != f["fate"]))}
     st = f["stats"]
-    flops = st["attempts"] * F_ATTEMPT + st["march_steps"] * F_RK4 + st["clamp_evals"] * F_EVAL + \
+    # the clamp reuses the step's first right-hand side: no FLOPs of its own
+    flops = st["attempts"] * F_ATTEMPT_EXEC + st["rays"] * F_EVAL + st["march_steps"] * F_RK4 + \
         st["bin_updates"] * F_BIN
     kms = f["phase_ms"][0]
     ach = flops / (kms * 1e-3) / 1e12
@@ -439,8 +444,9 @@ def run_volumetric(args, torch, G, stream, flush, p64):
            "speedup_mixed_vs_fp64": f["ms_per_step"] / m["ms_per_step"], "mixed_error_vs_fp64": err,
            "roofline_fp64": {"kernel": "vol_spectral_kernel<false>", "bound": "fp64", "achieved": ach, "peak": p64,
                              "unit": "TFLOP/s", "frac": ach / p64,
-                             "flop_count": f"{F_ATTEMPT}/attempt, {F_RK4}/march step, {F_EVAL}/clamp, "
-                                           f"{F_BIN}/bin update (transcendentals not counted), device counters"},
+                             "flop_count": f"{F_ATTEMPT_EXEC}/attempt + {F_EVAL}/ray (first right-hand side), "
+                                           f"{F_RK4}/march step, {F_BIN}/bin update (transcendentals and the "
+                                           f"right-hand sides after march ends not counted), device counters"},
            "cube_store": {"bytes": cube, "GB_per_s": cube / (kms * 1e-3) / 1e9}}
     if not args.no_cpu_baseline:
         try:
@@ -684,7 +690,7 @@ def main():
                            "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])}
         # FP64 form: thin_render_kernel, FP64 FLOPs against the DGEMM peak
         st64 = res[G.FORM_FP64]["stats"]
-        fl64 = st64["attempts"] * F_ATTEMPT
+        fl64 = st64["attempts"] * F_ATTEMPT_EXEC + RAYS * F_EVAL
         a64 = fl64 / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
         forms["fp64"]["roofline"] = {"kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": a64,
                                      "peak": p64, "unit": "TFLOP/s", "frac": a64 / p64}
@@ -693,8 +699,8 @@ def main():
         stm = res[G.FORM_MIXED]["stats"]
         ph = res[G.FORM_MIXED]["phase_ms"]
         spec_att = stm["attempts"] - stm["fp64_attempts"]
-        a_spec = spec_att * F_ATTEMPT / (ph[0] * 1e-3) / 1e12
-        a_re = stm["fp64_attempts"] * F_ATTEMPT / (ph[2] * 1e-3) / 1e12
+        a_spec = (spec_att * F_ATTEMPT_EXEC + RAYS * F_EVAL) / (ph[0] * 1e-3) / 1e12
+        a_re = stm["fp64_attempts"] * F_ATTEMPT_EXEC / (ph[2] * 1e-3) / 1e12
         forms["mixed"]["phases"] = ["mixed_speculate_kernel", "mixed_star_kernel", "mixed_retrace_kernel",
                                     "mixed_resolve_kernel"]
         forms["mixed"]["roofline"] = {
@@ -702,17 +708,19 @@ def main():
             "retrace": {"bound": "fp64", "achieved": a_re, "peak": p64, "unit": "TFLOP/s", "frac": a_re / p64}}
         if head_form == G.FORM_MIXED:
             roof = dict(forms["mixed"]["roofline"]["speculate"])
-            roof.update(kernel="mixed_speculate_kernel", flops_per_launch=spec_att * F_ATTEMPT,
-                        flop_count=f"{F_ATTEMPT} per DP45 attempt (FP32 stages) x {spec_att} speculative attempts "
-                                   f"(device counter)",
+            roof.update(kernel="mixed_speculate_kernel", flops_per_launch=spec_att * F_ATTEMPT_EXEC + RAYS * F_EVAL,
+                        flop_count=f"{F_ATTEMPT_EXEC} per DP45 attempt (FP32 stages, first right-hand side kept "
+                                   f"from the previous attempt) x {spec_att} speculative attempts (device counter) "
+                                   f"+ {F_EVAL} per ray",
                         peak_source="cuBLAS SGEMM 8192^3, TF32 off, measured in this run (best of 5); "
                                     "MEASURED_PEAKS.json has no FP32 figure",
                         launch_ms=ph[0], traffic=None)
             launches = args.steps * (4 if params["background_type"] == G.BG_STARS else 3)
         else:
             roof = dict(forms["fp64"]["roofline"])
-            roof.update(flops_per_launch=fl64, flop_count=f"{F_ATTEMPT} per DP45 attempt x {st64['attempts']} "
-                                                          f"attempts (device counter)",
+            roof.update(flops_per_launch=fl64, flop_count=f"{F_ATTEMPT_EXEC} per DP45 attempt (first right-hand "
+                                                          f"side kept from the previous attempt) x {st64['attempts']} "
+                                                          f"attempts (device counter) + {F_EVAL} per ray",
                         peak_source="cuBLAS FP64 GEMM 8192^3 measured in this run (best of 5); MEASURED_PEAKS.json "
                                     "has no FP64 figure", traffic=None)
             launches = args.steps

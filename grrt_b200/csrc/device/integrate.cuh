@@ -46,11 +46,16 @@ GRRT_HD Vec5<T> rk4_step(T M, T a, T pt, T pph, const Vec5<T>& y, T h) {
 #undef GRRT_RK4C
 }
 
-// One DP45 attempt: returns the 5th-order state in y5 and the error norm.
+// One DP45 attempt with k1 = f(y) given by the caller: returns the error
+// norm, the 5th-order state in y5 and k7 = f(y5). The reference evaluates
+// f(y) afresh at every attempt; it is the same value as the previous accepted
+// attempt's k7 (same state, same constants) or the rejected attempt's k1
+// (same state), so a caller that keeps it evaluates six right-hand sides per
+// attempt instead of seven with identical results.
 template <typename T>
-GRRT_HD T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5) {
+GRRT_HD T dp45_attempt_k1(T M, T a, T pt, T pph, const Vec5<T>& y, T h, const Vec5<T>& k1, Vec5<T>& y5,
+                          Vec5<T>& k7_out) {
     using namespace dp;
-    const Vec5<T> k1 = kerr_rhs<T>(M, a, pt, pph, y);
 #define GRRT_S2(f) y.f + h * (T(a21) * k1.f)
     const Vec5<T> k2 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{GRRT_S2(r), GRRT_S2(th), GRRT_S2(ph), GRRT_S2(pr), GRRT_S2(pth)});
 #define GRRT_S3(f) y.f + h * (T(a31) * k1.f + T(a32) * k2.f)
@@ -73,6 +78,7 @@ GRRT_HD T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5
 #undef GRRT_Y5
 #undef GRRT_E6
     const Vec5<T> k7 = kerr_rhs<T>(M, a, pt, pph, y5);
+    k7_out = k7;
     // err = max |h (sum e_i k_i)| / (|y5| + 1e-10); max written as the
     // standard library's (a < b) ? b : a so a NaN term is skipped as there.
     T err = T(0);
@@ -86,18 +92,34 @@ GRRT_HD T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5
     return err;
 }
 
+// One DP45 attempt from scratch: returns the 5th-order state in y5 and the error norm.
+template <typename T>
+GRRT_HD T dp45_attempt(T M, T a, T pt, T pph, const Vec5<T>& y, T h, Vec5<T>& y5) {
+    const Vec5<T> k1 = kerr_rhs<T>(M, a, pt, pph, y);
+    Vec5<T> k7;
+    return dp45_attempt_k1<T>(M, a, pt, pph, y, h, k1, y5, k7);
+}
+
+// f(y) in FP32 as the mixed-precision attempt forms it (state rounded to FP32).
+GRRT_HD Vec5<float> mixed_k1(float M, float a, float pt, float pph, const Vec5<double>& y) {
+    const Vec5<float> yf{static_cast<float>(y.r), static_cast<float>(y.th), static_cast<float>(y.ph),
+                         static_cast<float>(y.pr), static_cast<float>(y.pth)};
+    return kerr_rhs<float>(M, a, pt, pph, yf);
+}
+
 // Mixed-precision attempt: the seven right-hand sides and the stage sums in
 // FP32, the state and its update in FP64 (y5 = y + double(h * sum b_i k_i)),
 // so round-off does not accumulate along the ray. The error norm is formed in
 // FP32; its noise floor (about 1e-7 of |h k|/|y|) is why FP32 steps are
 // controlled against their own tolerance (DevScene::tol_fp32).
-GRRT_HD double mixed_attempt_impl(float M, float a, float pt, float pph, const Vec5<double>& y, double dl,
-                                  Vec5<double>& y5, Vec5<float>& k7_out) {
+// k1 = mixed_k1(y) is given by the caller (the previous accepted attempt's
+// k7, which is f at float(y5) = float(new y), or the rejected attempt's k1).
+GRRT_HD double mixed_attempt_k1(float M, float a, float pt, float pph, const Vec5<double>& y, double dl,
+                                const Vec5<float>& k1, Vec5<double>& y5, Vec5<float>& k7_out) {
     using namespace dp;
     const Vec5<float> yf{static_cast<float>(y.r), static_cast<float>(y.th), static_cast<float>(y.ph),
                          static_cast<float>(y.pr), static_cast<float>(y.pth)};
     const float h = static_cast<float>(dl);
-    const Vec5<float> k1 = kerr_rhs<float>(M, a, pt, pph, yf);
 #define GRRT_F(expr_r, expr_th, expr_ph, expr_pr, expr_pth) Vec5<float>{expr_r, expr_th, expr_ph, expr_pr, expr_pth}
 #define GRRT_ST(f, comb) yf.f + h * (comb)
 #define GRRT_C2(f) float(a21) * k1.f
@@ -137,6 +159,11 @@ GRRT_HD double mixed_attempt_impl(float M, float a, float pt, float pph, const V
     GRRT_ERRF(r) GRRT_ERRF(th) GRRT_ERRF(ph) GRRT_ERRF(pr) GRRT_ERRF(pth)
 #undef GRRT_ERRF
     return static_cast<double>(err);
+}
+
+GRRT_HD double mixed_attempt_impl(float M, float a, float pt, float pph, const Vec5<double>& y, double dl,
+                                  Vec5<double>& y5, Vec5<float>& k7_out) {
+    return mixed_attempt_k1(M, a, pt, pph, y, dl, mixed_k1(M, a, pt, pph, y), y5, k7_out);
 }
 
 // Outcome of the controller after one attempt (src/rk4.cpp:87-136).

@@ -155,6 +155,8 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
     unsigned q = ~0u;
     bool live = false, exhausted = false;
     Vec5<double> y;
+    Vec5<float> k1;  // FP32 f(y), kept from the previous attempt when k1_ok
+    bool k1_ok = false;
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0;
     mixed::Tracker trk;
@@ -174,6 +176,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
+                k1_ok = false;
                 if (kBatch)
                     trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.fp32_r_min);
                 else
@@ -187,15 +190,20 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
         Vec5<float> k7;
         if (live && retry == 0) term = start_test(S, step, y.r);
         if (live && term < 0) {
+            if (!k1_ok) {
+                k1 = mixed_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y);
+                k1_ok = true;
+            }
             Vec5<double> y5;
             const double err =
-                mixed_attempt_impl(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, y5, k7);
+                mixed_attempt_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, k1, y5, k7);
             ++n_att;
             const StepDecision d = pi_control(err, S.tol_fp32, dl, retry, y5.r);
             if (d.accept) {
                 ++n_acc;
                 retrace = trk.step(y, y5);
                 y = y5;
+                k1 = k7;
                 dl = d.next;
                 retry = 0;
                 ++step;
@@ -278,7 +286,8 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
     unsigned long long n_att = 0, n_acc = 0;
     unsigned q = ~0u;
     bool live = false, exhausted = false;
-    Vec5<double> y;
+    Vec5<double> y, k1;  // k1 = f(y), kept from the previous attempt when k1_ok
+    bool k1_ok = false;
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0, ncross = 0;
     double c0 = 0, c1 = 0, c2 = 0;
@@ -296,6 +305,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
                 step = 0;
                 ncross = 0;
                 c0 = c1 = c2 = 0.0;
+                k1_ok = false;
                 live = true;
             }
         }
@@ -303,8 +313,12 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
         int term = -1;
         if (live && retry == 0) term = start_test(S, step, y.r);
         if (live && term < 0) {
-            Vec5<double> y5;
-            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            if (!k1_ok) {
+                k1 = kerr_rhs<double>(S.M, S.a, pt, pph, y);
+                k1_ok = true;
+            }
+            Vec5<double> y5, k7;
+            const double err = dp45_attempt_k1<double>(S.M, S.a, pt, pph, y, dl, k1, y5, k7);
             ++n_att;
             const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
             if (d.accept) {
@@ -326,6 +340,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
                     }
                 }
                 y = y5;
+                k1 = k7;
                 dl = d.next;
                 retry = 0;
                 ++step;

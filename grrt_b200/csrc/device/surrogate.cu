@@ -109,7 +109,8 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
     unsigned q = ~0u;
     bool live = false, exhausted = false;
     const DevScene* S = scenes;
-    Vec5<double> y;
+    Vec5<double> y, k1;  // k1 = f(y), kept from the previous attempt when k1_ok
+    bool k1_ok = false;
     double pt = 0, pph = 0, dl = 0, r1 = 0, r2 = 0;
     int retry = 0, step = 0, nc = 0, n_extra = 0;
     while (true) {
@@ -143,6 +144,7 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
                 nc = 0;
                 n_extra = 0;
                 r1 = r2 = 0.0;
+                k1_ok = false;
                 live = true;
             }
         }
@@ -154,8 +156,12 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
             else if (y.r > S->r_escape) term = kTermEscaped;
         }
         if (live && term < 0) {
-            Vec5<double> y5;
-            const double err = dp45_attempt<double>(S->M, S->a, pt, pph, y, dl, y5);
+            if (!k1_ok) {
+                k1 = kerr_rhs<double>(S->M, S->a, pt, pph, y);
+                k1_ok = true;
+            }
+            Vec5<double> y5, k7;
+            const double err = dp45_attempt_k1<double>(S->M, S->a, pt, pph, y, dl, k1, y5, k7);
             ++n_att;
             const StepDecision d = pi_control(err, S->tol, dl, retry, y5.r);
             if (d.accept) {
@@ -172,6 +178,7 @@ surr_trace_kernel(const DevScene* __restrict__ scenes, int n_cams, int n_side, i
                     ++nc;
                 }
                 y = y5;
+                k1 = k7;
                 dl = d.next;
                 retry = 0;
                 ++step;

@@ -97,6 +97,8 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
     // ray slot
     bool live = false;
     Vec5<double> y;      // state at the start of the current outer step
+    Vec5<double> k1;     // f(y), kept from the previous attempt when k1_ok
+    bool k1_ok = false;
     double pt = 0.0, pph = 0.0;
     double dl = 0.0, dlambda = 0.0;
     int retry = 0, step = 0, ncross = 0;
@@ -162,6 +164,7 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
             step = 0;
             ncross = 0;
             col0 = col1 = col2 = 0.0;
+            k1_ok = false;
             live = true;
         }
         int term = -1;
@@ -169,8 +172,12 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
 
         // ---- one DP45 attempt for every lane with a live, unterminated ray ----
         if (live && term < 0) {
-            Vec5<double> y5;
-            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            if (!k1_ok) {
+                k1 = kerr_rhs<double>(S.M, S.a, pt, pph, y);
+                k1_ok = true;
+            }
+            Vec5<double> y5, k7;
+            const double err = dp45_attempt_k1<double>(S.M, S.a, pt, pph, y, dl, k1, y5, k7);
             ++cnt.fp64_attempts;
             ++cnt.attempts;
             const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
@@ -197,6 +204,7 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
                     }
                 }
                 y = y5;
+                k1 = k7;
                 dlambda = d.next;
                 dl = dlambda;
                 retry = 0;

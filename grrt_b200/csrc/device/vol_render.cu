@@ -51,6 +51,8 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
     double acc[3] = {0.0, 0.0, 0.0};
     bool live = false, need_start = false, marching = false;
     Vec5<double> y{}, prev{};
+    Vec5<double> k1{};  // f(y) while k1_ok: the last accepted attempt's k7 or this step's first stage
+    bool k1_ok = false;
     double pt = 0.0, pph = 0.0, dl = 0.0, dlambda = 0.0;
     int retry = 0, step = 0, entries = 0;
     // transfer state (RGB in registers)
@@ -100,6 +102,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             marching = false;
             J[0] = J[1] = J[2] = 0.0;
             Tt[0] = Tt[1] = Tt[2] = 1.0;
+            k1_ok = false;
             live = true;
             need_start = true;
         }
@@ -111,7 +114,11 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             else if (y.r < S.r_stop) term = kTermHorizon;
             else if (y.r > S.r_escape) term = kTermEscaped;
             if (term < 0) {
-                if (vol_clamp(S, pt, pph, y, dlambda)) ++cnt.clamp;
+                if (!k1_ok) {
+                    k1 = kerr_rhs<double>(S.M, S.a, pt, pph, y);
+                    k1_ok = true;
+                }
+                if (vol_clamp(S, k1, y, dlambda)) ++cnt.clamp;
                 prev = y;
                 dl = dlambda;
                 retry = 0;
@@ -121,8 +128,8 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
 
         if (live && term < 0 && !marching) {
             // ---- one DP45 attempt ----
-            Vec5<double> y5;
-            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            Vec5<double> y5, k7;
+            const double err = dp45_attempt_k1<double>(S.M, S.a, pt, pph, y, dl, k1, y5, k7);
             ++cnt.fp64;
             ++cnt.attempts;
             const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
@@ -132,6 +139,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             } else {
                 ++cnt.accepted;
                 y = y5;
+                k1 = k7;
                 dlambda = d.next;
                 ++step;  // the reference's loop counter advances on every outer iteration
                 // hand-over to the ray-march (src/geodesic_tracer.cpp:105-153)
@@ -214,6 +222,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             if (end) {
                 marching = false;
                 y = ms;  // the outer loop continues from the march's end state
+                k1_ok = false;
                 need_start = true;
             }
         }

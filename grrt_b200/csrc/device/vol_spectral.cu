@@ -75,6 +75,8 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
     int pix = -1, smp = 0;  // kList: pix = the listed sample
     bool live = false, need_start = false, marching = false;
     Vec5<double> y{}, prev{};
+    Vec5<double> k1{};  // f(y) while k1_ok: the last accepted attempt's k7 or this step's first stage
+    bool k1_ok = false;
     double pt = 0.0, pph = 0.0, dl = 0.0, dlambda = 0.0;
     int retry = 0, step = 0, entries = 0, n_thick = 0;
     Vec5<double> ms{};
@@ -123,6 +125,7 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             entries = 0;
             marching = false;
             n_thick = 0;
+            k1_ok = false;
             live = true;
             need_start = true;
             fresh_ray = true;
@@ -151,7 +154,11 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             else if (y.r < S.r_stop) term = kTermHorizon;
             else if (y.r > S.r_escape) term = kTermEscaped;
             if (term < 0) {
-                if (vol_clamp(S, pt, pph, y, dlambda)) ++cnt.clamp;
+                if (!k1_ok) {
+                    k1 = kerr_rhs<double>(S.M, S.a, pt, pph, y);
+                    k1_ok = true;
+                }
+                if (vol_clamp(S, k1, y, dlambda)) ++cnt.clamp;
                 prev = y;
                 dl = dlambda;
                 retry = 0;
@@ -168,8 +175,8 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
         Vec5<double> ns{};
         if (live && term < 0 && !marching) {
             // ---- one DP45 attempt ----
-            Vec5<double> y5;
-            const double err = dp45_attempt<double>(S.M, S.a, pt, pph, y, dl, y5);
+            Vec5<double> y5, k7;
+            const double err = dp45_attempt_k1<double>(S.M, S.a, pt, pph, y, dl, k1, y5, k7);
             ++cnt.fp64;
             ++cnt.attempts;
             const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
@@ -179,6 +186,7 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             } else {
                 ++cnt.accepted;
                 y = y5;
+                k1 = k7;
                 dlambda = d.next;
                 ++step;  // the reference's loop counter advances on every outer iteration
                 // hand-over to the ray-march (src/geodesic_tracer.cpp:105-153)
@@ -299,6 +307,7 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             if (mend) {
                 marching = false;
                 y = ms;  // the outer loop continues from the march's end state
+                k1_ok = false;
                 need_start = true;
             }
         }
@@ -472,6 +481,8 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
     int retry = 0, step = 0;
     mixed::Tracker trk;
     ReachRay rr;
+    Vec5<float> k1;  // FP32 f(y), kept from the previous attempt when k1_ok
+    bool k1_ok = false;
     while (true) {
         const bool want = !live && !exhausted;
         const unsigned m = __ballot_sync(kWarp, want);
@@ -502,6 +513,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
                 retry = 0;
                 step = 0;
                 trk.reset(false, 0.0, 0.0, 0.0, S.fp32_r_min);
+                k1_ok = false;
                 live = true;
             }
         }
@@ -514,16 +526,21 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
             else if (y.r > S.r_escape) term = kTermEscaped;
         }
         if (live && term < 0) {
+            if (!k1_ok) {
+                k1 = mixed_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y);
+                k1_ok = true;
+            }
             Vec5<double> y5;
             Vec5<float> k7;
             const double err =
-                mixed_attempt_impl(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, y5, k7);
+                mixed_attempt_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, k1, y5, k7);
             ++cnt.attempts;
             const StepDecision d = pi_control(err, S.tol_fp32, dl, retry, y5.r);
             if (d.accept) {
                 ++cnt.accepted;
                 retrace = vol_reach(reach, rr, y, y5) || trk.step(y, y5);
                 y = y5;
+                k1 = k7;
                 dl = d.next;
                 retry = 0;
                 ++step;

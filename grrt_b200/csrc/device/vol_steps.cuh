@@ -47,9 +47,10 @@ __device__ __forceinline__ double add_intensity(double sum, double J, double f) 
 
 // Near-disk clamp at the start of an outer step (src/geodesic_tracer.cpp:71-95):
 // for r in [0.9 r_h, 1.5 r_outer] and |z| < z_max + 6 H, dlambda is capped at
-// max(H / (4 |dz/dlambda|), H / 64). Returns whether it evaluated the
-// right-hand side (the clamp counter).
-__device__ __forceinline__ bool vol_clamp(const DevScene& S, double pt, double pph, const Vec5<double>& y,
+// max(H / (4 |dz/dlambda|), H / 64). d = f(y), the right-hand side the step's
+// first DP45 stage uses too (the reference evaluates it here once more).
+// Returns whether the clamp applied (the clamp counter).
+__device__ __forceinline__ bool vol_clamp(const DevScene& S, const Vec5<double>& d, const Vec5<double>& y,
                                           double& dlambda) {
     const DevVolume& V = S.vol;
     const double r = y.r;
@@ -60,7 +61,6 @@ __device__ __forceinline__ bool vol_clamp(const DevScene& S, double pt, double p
     const double H = v_scale_height(V, r);
     const double zm = v_zmax(V, r);
     if (!(fabs(z) < zm + 6.0 * H)) return false;
-    const Vec5<double> d = kerr_rhs<double>(S.M, S.a, pt, pph, y);
     const double dz_dl = fabs(ct * d.r - r * st * d.th);
     if (dz_dl > 1e-20) {
         const double dl_max = vmax(0.25 * H / dz_dl, H / 64.0);

@@ -82,6 +82,77 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
     return mixed::star_in_reach(st, mixed::escape_arc(r_esc, y, k7)) ? 1 : 0;
 }
 
+// A full adaptive trace of one camera ray to termination with the FP64 DP45
+// attempt (mode bit 1 clear) or the FP32 mixed attempt (bit 1 set), taking k1
+// from the previous attempt (bit 0 set) or evaluating it afresh every attempt
+// (bit 0 clear), as the kernels do. sc = (M, a, r_stop, r_escape, dl0, tol,
+// max_steps). out8 = (termination, accepted steps, attempts, r, theta, phi,
+// p_r, p_theta) at the end.
+void devmath_trace_final(const double* sc, const double* y8, int mode, double* out8) {
+    const double M = sc[0], a = sc[1], r_stop = sc[2], r_esc = sc[3], dl0 = sc[4], tol = sc[5];
+    const int max_steps = static_cast<int>(sc[6]);
+    const bool reuse = (mode & 1) != 0, f32 = (mode & 2) != 0;
+    const double pt = y8[4], pph = y8[7];
+    Vec5<double> y{y8[1], y8[2], y8[3], y8[5], y8[6]};
+    Vec5<double> k1{};
+    Vec5<float> k1f{};
+    bool k1_ok = false;
+    double dl = dl0;
+    int retry = 0, step = 0, attempts = 0, term = -1;
+    while (true) {
+        if (retry == 0) {
+            if (step >= max_steps) { term = kTermMaxSteps; break; }
+            if (y.r < r_stop) { term = kTermHorizon; break; }
+            if (y.r > r_esc) { term = kTermEscaped; break; }
+        }
+        Vec5<double> y5;
+        double err;
+        if (f32) {
+            Vec5<float> k7;
+            if (!reuse || !k1_ok) k1f = mixed_k1(float(M), float(a), float(pt), float(pph), y);
+            err = mixed_attempt_k1(float(M), float(a), float(pt), float(pph), y, dl, k1f, y5, k7);
+            k1_ok = reuse;
+            const StepDecision d = pi_control(err, tol, dl, retry, y5.r);
+            ++attempts;
+            if (d.accept) {
+                y = y5;
+                k1f = k7;
+                dl = d.next;
+                retry = 0;
+                ++step;
+            } else {
+                dl = d.next;
+                ++retry;
+            }
+        } else {
+            Vec5<double> k7;
+            if (!reuse || !k1_ok) k1 = kerr_rhs<double>(M, a, pt, pph, y);
+            err = dp45_attempt_k1<double>(M, a, pt, pph, y, dl, k1, y5, k7);
+            k1_ok = reuse;
+            const StepDecision d = pi_control(err, tol, dl, retry, y5.r);
+            ++attempts;
+            if (d.accept) {
+                y = y5;
+                k1 = k7;
+                dl = d.next;
+                retry = 0;
+                ++step;
+            } else {
+                dl = d.next;
+                ++retry;
+            }
+        }
+    }
+    out8[0] = term;
+    out8[1] = step;
+    out8[2] = attempts;
+    out8[3] = y.r;
+    out8[4] = y.th;
+    out8[5] = y.ph;
+    out8[6] = y.pr;
+    out8[7] = y.pth;
+}
+
 // Closed-form margins of the surrogate for a camera ray y8 = (t, r, th, ph,
 // p_t, p_r, p_th, p_ph): out2 = (capture margin, graze margin).
 void devmath_ray_margins(double M, double a, double r_h, const double* y8, double* out2) {

@@ -30,6 +30,7 @@ def devmath():
     L.devmath_rhs_f32.argtypes = [C.c_double, C.c_double, PD, PD]
     L.devmath_dp45.restype = C.c_double
     L.devmath_dp45.argtypes = [C.c_double, C.c_double, PD, C.c_double, PD]
+    L.devmath_trace_final.argtypes = [PD, PD, C.c_int, PD]
     return L
 
 
@@ -93,3 +94,29 @@ def test_dp45_step_matches_oracle_trajectory(grrt, oracle_lib, devmath):
     # against an RK4-resolved solution of the same ODE instead
     assert 0.0 <= err < 1e-6
     assert abs(y5[0] - y[1]) < 1.0 and np.all(np.isfinite(y5))
+
+
+@pytest.mark.parametrize("f32", [False, True], ids=["fp64", "fp32-mixed"])
+def test_k1_reuse_traces_identically(grrt, oracle_lib, devmath, f32):
+    """The kernels take each attempt's k1 = f(y) from the previous attempt
+    (k7 after an accept, the same k1 after a reject) instead of evaluating it
+    again: whole traces must come out bit for bit the same as with a fresh
+    k1 every attempt, including the attempt and step counts."""
+    R = grrt.Renderer(grrt.config_params(2, width=64, height=64))
+    O = oracle_lib.Oracle(R)
+    s = R.table("scalars")
+    M, a, r_h, r_obs, tol, max_steps = s[0], s[1], s[2], s[4], s[5], s[6]
+    sc = np.array([M, a, r_h + 0.01, 1000.0, 0.01 * r_obs, 1e-6 if f32 else tol, max_steps])
+    rng = np.random.default_rng(11)
+    mode = 2 if f32 else 0
+    n_rejects = 0
+    for x, y in zip(rng.uniform(0, 64, 24), rng.uniform(0, 64, 24)):
+        y8 = np.ascontiguousarray(O.camera_ray(x, y))
+        fresh, kept = np.zeros(8), np.zeros(8)
+        devmath.devmath_trace_final(sc.ctypes.data_as(C.POINTER(C.c_double)), y8.ctypes.data_as(C.POINTER(C.c_double)),
+                                    mode, fresh.ctypes.data_as(C.POINTER(C.c_double)))
+        devmath.devmath_trace_final(sc.ctypes.data_as(C.POINTER(C.c_double)), y8.ctypes.data_as(C.POINTER(C.c_double)),
+                                    mode | 1, kept.ctypes.data_as(C.POINTER(C.c_double)))
+        np.testing.assert_array_equal(kept, fresh)
+        n_rejects += int(fresh[2] - fresh[1])
+    assert n_rejects > 0  # the reject path was exercised
