@@ -48,10 +48,13 @@ GRRT_HD Vec5<T> rk4_step(T M, T a, T pt, T pph, const Vec5<T>& y, T h) {
 
 // One DP45 attempt with k1 = f(y) given by the caller: returns the error
 // norm, the 5th-order state in y5 and k7 = f(y5). The reference evaluates
-// f(y) afresh at every attempt; it is the same value as the previous accepted
+// f(y) afresh at every attempt; mathematically it is the previous accepted
 // attempt's k7 (same state, same constants) or the rejected attempt's k1
 // (same state), so a caller that keeps it evaluates six right-hand sides per
-// attempt instead of seven with identical results.
+// attempt instead of seven. Without FMA contraction the kept value is
+// bit-identical to a fresh one; the device compiler may contract each inlined
+// copy of the right-hand side differently, so on the GPU the two can differ
+// in the last bits (the method and its step decisions are unchanged).
 template <typename T>
 GRRT_HD T dp45_attempt_k1(T M, T a, T pt, T pph, const Vec5<T>& y, T h, const Vec5<T>& k1, Vec5<T>& y5,
                           Vec5<T>& k7_out) {

@@ -100,8 +100,9 @@ def test_dp45_step_matches_oracle_trajectory(grrt, oracle_lib, devmath):
 def test_k1_reuse_traces_identically(grrt, oracle_lib, devmath, f32):
     """The kernels take each attempt's k1 = f(y) from the previous attempt
     (k7 after an accept, the same k1 after a reject) instead of evaluating it
-    again: whole traces must come out bit for bit the same as with a fresh
-    k1 every attempt, including the attempt and step counts."""
+    again. Built without FMA contraction (as here), whole traces must come out
+    bit for bit the same as with a fresh k1 every attempt, including the
+    attempt and step counts: the bookkeeping keeps exactly f(y)."""
     R = grrt.Renderer(grrt.config_params(2, width=64, height=64))
     O = oracle_lib.Oracle(R)
     s = R.table("scalars")
