@@ -571,8 +571,10 @@ def run_surrogate(args, torch, G, stream, flush, peaks):
         "fp64": {"value": rays / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64},
         "mixed": {"value": rays / (ms_mixed * 1e-3), "ms_per_step": ms_mixed},
         "speedup_vs_fp64": ms_fp64 / ms_surr, "speedup_vs_mixed": ms_mixed / ms_surr,
-        "phase_ms": {"network_and_shading": phases[0], "exact_retrace": phases[2], "resolve": phases[3]},
+        "phase_ms": {"network_and_shading": phases[0], "fp32_speculation": phases[1], "exact_retrace": phases[2],
+                     "resolve": phases[3]},
         "exact_fraction": exact / max(1, samples),
+        "speculated_fraction": S.last_counts()["speculated"] / max(1, samples),
         "attempts": {"surrogate": st["attempts"], "fp64": st64["attempts"]},
         "error_vs_fp64": {"max_rel": float(rel.max()), "pixels_over_1e-3": int((rel > 1e-3).sum()),
                           "lit_pixels": int(lit.sum()),

@@ -98,6 +98,7 @@ struct GRRTSurrogate {
     LossWeights weights;
     size_t last_render_samples = 0;
     const unsigned* last_retrace_count = nullptr;
+    const unsigned* last_spec_count = nullptr;
 
     ~GRRTSurrogate() {
         if (device >= 0) cudaSetDevice(device);
@@ -544,6 +545,7 @@ struct GRRTSurrogate {
         cudaEventDestroy(e_out);
         last_render_samples = n;
         last_retrace_count = mb.retrace_count;
+        last_spec_count = mb.spec_count;
         return true;
     }
 
@@ -860,17 +862,25 @@ extern "C" GRRT_EXPORT int grrt_surrogate_load(GRRTSurrogate* s, const char* pat
     return 0;
 }
 
-extern "C" GRRT_EXPORT int grrt_surrogate_last_exact(const GRRTSurrogate* s, long long* exact, long long* samples) {
+extern "C" GRRT_EXPORT int grrt_surrogate_last_counts(const GRRTSurrogate* s, long long* exact,
+                                                      long long* speculated, long long* samples) {
     if (!s || !exact || !samples) return -1;
-    unsigned h = 0;
-    if (s->last_retrace_count) {
+    unsigned h[2] = {0, 0};
+    const unsigned* src[2] = {s->last_retrace_count, s->last_spec_count};
+    for (int k = 0; k < 2; ++k) {
+        if (!src[k]) continue;
         cudaSetDevice(s->device);
-        if (s->copy(&h, s->last_retrace_count, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (s->copy(&h[k], src[k], sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) {
             cudaGetLastError();
             return -1;
         }
     }
-    *exact = h;
+    *exact = h[0];
+    if (speculated) *speculated = h[1];
     *samples = static_cast<long long>(s->last_render_samples);
     return 0;
+}
+
+extern "C" GRRT_EXPORT int grrt_surrogate_last_exact(const GRRTSurrogate* s, long long* exact, long long* samples) {
+    return grrt_surrogate_last_counts(s, exact, nullptr, samples);
 }

@@ -118,6 +118,9 @@ GRRT_EXPORT int grrt_surrogate_render_device(GRRTSurrogate* s, GRRTContext* ctx,
 GRRT_EXPORT int grrt_surrogate_render(GRRTSurrogate* s, GRRTContext* ctx, float* framebuffer);
 /* Samples re-traced exactly and samples in the last render (the context must still exist). */
 GRRT_EXPORT int grrt_surrogate_last_exact(const GRRTSurrogate* s, long long* exact, long long* samples);
+/* The same, plus the samples sent to the FP32 speculation (speculated may be NULL). */
+GRRT_EXPORT int grrt_surrogate_last_counts(const GRRTSurrogate* s, long long* exact, long long* speculated,
+                                           long long* samples);
 
 GRRT_EXPORT int grrt_surrogate_save(const GRRTSurrogate* s, const char* path);
 GRRT_EXPORT int grrt_surrogate_load(GRRTSurrogate* s, const char* path);
