@@ -208,6 +208,14 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                 retry = 0;
                 ++step;
                 term = retrace ? kTermMaxSteps : start_test(S, step, y.r);
+                // black sky: an escape is final as soon as it is certain
+                if (term < 0 && !S.stars_on) {
+                    const double m = kBatch ? S.mixed_margin : mb.margin;
+                    const double r_near = kBatch ? S.fp32_r_min : mb.r_near;
+                    const double r_min = fmax(fmax(mixed::kEscapeRMin * S.M, r_near),
+                                              S.disk_on ? S.r_out + 2.0 * m : 0.0);
+                    if (mixed::certain_escape(y, r_min, step, S.max_steps)) term = kTermEscaped;
+                }
             } else {
                 dl = d.next;
                 ++retry;

@@ -41,6 +41,20 @@ constexpr double kPi = 3.14159265358979323846;
 // sample_fate value of an escape whose star test is still to run.
 constexpr unsigned kFateStarPending = 0xffffffffu;
 
+// Early end of a speculative trace on a black sky: an outgoing ray (p_r > 0)
+// beyond r_min can no longer come back (a null geodesic turns back outward of
+// the photon orbits only at a radius below its outermost turning point, which
+// an outgoing ray has passed), so it escapes with no further disk crossing or
+// near-hole sweep, and with no star to look up its colour is already final.
+// r_min must lie outside the region the pass tests (disk radii plus margins,
+// r_near) and outside every photon orbit (kEscapeRMin >= 4 M for |a| <= M).
+// steps: the FP32 pass's accepted steps so far; the FP64 trace, which takes
+// more steps, must still be far from the step budget on its way out.
+constexpr double kEscapeRMin = 5.0;
+GRRT_HD bool certain_escape(const Vec5<double>& y, double r_min, int steps, int max_steps) {
+    return y.pr > 0.0 && y.r > r_min && 3 * steps + 1000 < max_steps;
+}
+
 struct Tracker {
     double lo = 0.0, hi = 0.0, r_near = 0.0;
     bool disk = false;

@@ -544,7 +544,13 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
                 dl = d.next;
                 retry = 0;
                 ++step;
-                if (retrace) term = kTermMaxSteps;
+                if (retrace)
+                    term = kTermMaxSteps;
+                else if (mixed::certain_escape(y,
+                                               fmax(fmax(mixed::kEscapeRMin * S.M, S.fp32_r_min),
+                                                    reach.R + 2.0 * reach.margin + 2e-3 * y.r),
+                                               step, S.max_steps))
+                    term = kTermEscaped;  // spectra carry no sky: the escape is final once certain
             } else {
                 dl = d.next;
                 ++retry;

@@ -66,6 +66,13 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
             dl = d.next;
             retry = 0;
             ++step;
+            // black sky: a certain escape is final (as mixed_speculate_kernel)
+            if (!stars_on && !(y.r > r_esc) &&
+                mixed::certain_escape(y, fmax(fmax(mixed::kEscapeRMin * M, sc[10]), disk_on ? sc[8] + 2.0 * sc[9] : 0.0),
+                                      step, max_steps)) {
+                *term_out = kTermEscaped;
+                return 0;
+            }
         } else {
             dl = d.next;
             ++retry;

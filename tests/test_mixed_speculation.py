@@ -57,6 +57,9 @@ CASES = [
     ("kerr 0.998 80deg stars", 2, 56, {}),
     ("kerr 0.998 edge-on stars", 2, 56, {"observer_theta": math.pi / 2}),
     ("kerr 0.5 30deg stars", 2, 48, {"spin": 0.5, "observer_theta": math.radians(30.0)}),
+    # black sky: certain escapes end the speculative trace early
+    ("kerr 0.998 80deg black sky", 2, 56, {"background_type": 0}),
+    ("kerr 0.9 edge-on black sky", 2, 48, {"spin": 0.9, "observer_theta": math.pi / 2, "background_type": 0}),
 ]
 
 
