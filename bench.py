@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--no-volumetric", action="store_true")
     ap.add_argument("--volumetric", action="store_true", help="run only the volumetric spectral section")
     ap.add_argument("--vol-size", type=int, default=512, help="volumetric frame side (profiler captures)")
+    # N > 1: "frames" renders one whole frame per GPU per step (weak scaling);
+    # "rows" splits one frame by interleaved rows and all-gathers it (strong scaling)
+    ap.add_argument("--shard", default="frames", choices=["frames", "rows"])
     return ap.parse_args()
 
 
@@ -313,9 +316,11 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def time_form(torch, R, form, stream, flush, rgba, steps, warmup, dist):
+def time_form(torch, R, form, stream, flush, render, steps, warmup, dist):
     """W warm-up frames, then K timed frames of one precision form: CUDA events
-    around each render launch on its stream, plus the library's per-phase events."""
+    around each frame's work (render(), enqueued on `stream`: the render
+    launches, and with rows sharded the all-gather), plus the library's
+    per-phase events."""
     R.set_precision(form)
 
     def step(ev=None):
@@ -323,7 +328,7 @@ def time_form(torch, R, form, stream, flush, rgba, steps, warmup, dist):
             flush.fill_(1.0)  # evict L2 between frames
             if ev is not None:
                 ev[0].record(stream)
-            R.render_device(rgba, None, None, stream)
+            render()
             if ev is not None:
                 ev[1].record(stream)
 
@@ -642,42 +647,71 @@ def main():
     stream = torch.cuda.Stream()
     rgba = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    rows = args.shard == "rows"
+    if rows:
+        # this rank's interleaved rows of the one frame, then the all-gather
+        row0, row_step, n_rows = G.multi.shard_rows(H, world, rank)
+        part = torch.empty((n_rows, W, 4), dtype=torch.float32, device="cuda")
+
+        def render():
+            R.render_rows_device(row0, row_step, n_rows, part, None, None, stream)
+            return G.multi.gather_frame(part, H, dist, world) if world > 1 else part
+        my_rays = n_rows * W * SPP
+        frames_per_step = 1
+    else:
+        def render():
+            R.render_device(rgba, None, None, stream)
+            return rgba
+        my_rays = RAYS
+        frames_per_step = world
 
     head_form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
     other_form = G.FORM_FP64 if head_form == G.FORM_MIXED else G.FORM_MIXED
     clocks = ClockSampler(local)
     clocks.start()
-    res = {other_form: time_form(torch, R, other_form, stream, flush, rgba, args.steps, args.warmup, dist),
-           head_form: time_form(torch, R, head_form, stream, flush, rgba, args.steps, args.warmup, dist)}
+    res = {other_form: time_form(torch, R, other_form, stream, flush, render, args.steps, args.warmup, dist),
+           head_form: time_form(torch, R, head_form, stream, flush, render, args.steps, args.warmup, dist)}
     clk = clocks.stop()
     head = res[head_form]
     ms = head["ms"]
-    value = world * RAYS / (ms * 1e-3)
+    value = frames_per_step * RAYS / (ms * 1e-3)
 
-    # end to end through the reference C entry point (host framebuffer), headline form
+    # end to end, headline form: whole frames through the reference C entry
+    # point (host framebuffer); with rows sharded, each rank's rows, the
+    # all-gather and rank 0's copy of the frame to the host
     host_fb = np.empty((H, W, 4), dtype=np.float32)
     import ctypes as C
     L = G.lib()
     fbp = host_fb.ctypes.data_as(C.POINTER(C.c_float))
+
+    def e2e_frame():
+        if rows:
+            with torch.cuda.stream(stream):
+                frame = render()
+            stream.synchronize()
+            if rank == 0:
+                host_fb[...] = frame.cpu().numpy()
+        else:
+            rc = L.grrt_render(R.ctx, fbp)
+            assert rc == 0, L.grrt_error(R.ctx)
     for _ in range(2):
-        L.grrt_render(R.ctx, fbp)
+        e2e_frame()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     e0 = time.perf_counter()
     e2e_steps = max(3, args.steps // 2)
     for _ in range(e2e_steps):
-        rc = L.grrt_render(R.ctx, fbp)
-        assert rc == 0, L.grrt_error(R.ctx)
+        e2e_frame()
     e2e_s = (time.perf_counter() - e0) / e2e_steps
     if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * RAYS / e2e_s, "unit": "rays/s",
+        e2e_s = G.multi.max_over_ranks(e2e_s, dist, "cuda")
+    e2e = {"value": frames_per_step * RAYS / e2e_s, "unit": "rays/s",
            "h2d_bytes_per_step": 1536,  # launch parameters (scene description) per frame
            "d2h_bytes_per_step": W * H * 16,  # float RGBA frame
-           "api": "grrt_render(ctx, float* host_framebuffer)", "form": args.form, "ms_per_step": 1e3 * e2e_s}
+           "api": ("grrt_render_rows_device + all-gather + copy to host" if rows
+                   else "grrt_render(ctx, float* host_framebuffer)"),
+           "form": args.form, "ms_per_step": 1e3 * e2e_s}
 
     if rank == 0:
         peaks = measured_peaks(torch)
@@ -687,12 +721,13 @@ def main():
         for name, form in (("fp64", G.FORM_FP64), ("mixed", G.FORM_MIXED)):
             r = res[form]
             st = r["stats"]
-            forms[name] = {"value": world * RAYS / (r["ms"] * 1e-3), "unit": "rays/s", "ms_per_step": r["ms"],
-                           "phase_ms": r["phase_ms"], "attempts_per_ray": st["attempts"] / RAYS,
+            forms[name] = {"value": frames_per_step * RAYS / (r["ms"] * 1e-3), "unit": "rays/s",
+                           "ms_per_step": r["ms"],
+                           "phase_ms": r["phase_ms"], "attempts_per_ray": st["attempts"] / my_rays,
                            "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])}
         # FP64 form: thin_render_kernel, FP64 FLOPs against the DGEMM peak
         st64 = res[G.FORM_FP64]["stats"]
-        fl64 = st64["attempts"] * F_ATTEMPT_EXEC + RAYS * F_EVAL
+        fl64 = st64["attempts"] * F_ATTEMPT_EXEC + my_rays * F_EVAL
         a64 = fl64 / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
         forms["fp64"]["roofline"] = {"kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": a64,
                                      "peak": p64, "unit": "TFLOP/s", "frac": a64 / p64}
@@ -701,7 +736,7 @@ def main():
         stm = res[G.FORM_MIXED]["stats"]
         ph = res[G.FORM_MIXED]["phase_ms"]
         spec_att = stm["attempts"] - stm["fp64_attempts"]
-        a_spec = (spec_att * F_ATTEMPT_EXEC + RAYS * F_EVAL) / (ph[0] * 1e-3) / 1e12
+        a_spec = (spec_att * F_ATTEMPT_EXEC + my_rays * F_EVAL) / (ph[0] * 1e-3) / 1e12
         a_re = stm["fp64_attempts"] * F_ATTEMPT_EXEC / (ph[2] * 1e-3) / 1e12
         forms["mixed"]["phases"] = ["mixed_speculate_kernel", "mixed_star_kernel", "mixed_retrace_kernel",
                                     "mixed_resolve_kernel"]
@@ -710,7 +745,7 @@ def main():
             "retrace": {"bound": "fp64", "achieved": a_re, "peak": p64, "unit": "TFLOP/s", "frac": a_re / p64}}
         if head_form == G.FORM_MIXED:
             roof = dict(forms["mixed"]["roofline"]["speculate"])
-            roof.update(kernel="mixed_speculate_kernel", flops_per_launch=spec_att * F_ATTEMPT_EXEC + RAYS * F_EVAL,
+            roof.update(kernel="mixed_speculate_kernel", flops_per_launch=spec_att * F_ATTEMPT_EXEC + my_rays * F_EVAL,
                         flop_count=f"{F_ATTEMPT_EXEC} per DP45 attempt (FP32 stages, first right-hand side kept "
                                    f"from the previous attempt) x {spec_att} speculative attempts (device counter) "
                                    f"+ {F_EVAL} per ray",
@@ -728,7 +763,7 @@ def main():
             launches = args.steps
         err = form_error(torch, G, params)
         cpu = None
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the CPU baseline is taken at N = 1 only
             try:
                 rays, secs, threads, kind, rows = cpu_reference_sample(0, 16)
                 cpu = {"value": rays / secs, "unit": "rays/s", "cores": threads, "kind": "reference",
@@ -738,27 +773,32 @@ def main():
                 cpu = {"value": None, "unit": "rays/s", "cores": os.cpu_count(), "kind": "reference",
                        "sample": f"unavailable: {ex}"}
         line = {"metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong" if rows else "weak",
                 "vs_baseline": None, "dtype": "f64" if head_form == G.FORM_FP64 else "f32+f64",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "rays_per_step": RAYS,
                            "form": args.form, "l2": "flushed between steps (256 MiB write)",
-                           "parallelism": f"one frame per GPU per step ({world} GPU)"},
+                           "parallelism": (f"one frame split by interleaved rows over {world} GPU, one "
+                                           f"all-gather per frame" if rows
+                                           else f"one frame per GPU per step ({world} GPU)")},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": launches, "forms": forms,
                 "speedup_mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
                 "mixed_error_vs_fp64": err,
-                "work": {"attempts_per_ray": head["stats"]["attempts"] / RAYS,
-                         "accepted_per_ray": head["stats"]["accepted"] / RAYS,
+                "work": {"attempts_per_ray": head["stats"]["attempts"] / my_rays,
+                         "accepted_per_ray": head["stats"]["accepted"] / my_rays,
                          "crossings": head["stats"]["crossings"],
                          "fp64_attempt_share": head["stats"]["fp64_attempts"] / max(1, head["stats"]["attempts"])},
                 "kernel_ms_per_step": head["kernel_ms"], "wall_s_timed_region": head["wall"]}
-        if not args.no_volumetric:
+        # the single-GPU sections run at N = 1 only (the other ranks would wait
+        # for them at the closing barrier)
+        if not args.no_volumetric and world == 1:
             try:
                 line["volumetric"] = run_volumetric(args, torch, G, stream, flush, p64)
             except Exception as ex:  # reported, the headline stands on its own
                 line["volumetric"] = {"error": str(ex)}
-        if args.surrogate_steps > 0:
+        if args.surrogate_steps > 0 and world == 1:
             try:
                 line["surrogate"] = run_surrogate(args, torch, G, stream, flush, peaks)
             except Exception as ex:  # reported, the headline stands on its own

@@ -21,7 +21,7 @@ import numpy as np
 
 __all__ = [
     "GRRTParams", "GRRTStats", "Renderer", "lib", "load_library", "build",
-    "FORM_FP64", "FORM_MIXED", "config_params", "LIB_PATH", "Surrogate",
+    "FORM_FP64", "FORM_MIXED", "config_params", "LIB_PATH", "Surrogate", "multi",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_get_precision": (C.c_int, [vp]),
         "grrt_set_mixed_params": (C.c_int, [vp, C.c_double, C.c_double]),
         "grrt_render_device": (C.c_int, [vp, vp, vp, vp, vp]),
+        "grrt_render_rows_device": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]),
         "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
@@ -310,6 +311,17 @@ class Renderer:
         s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
         self._check(self._L.grrt_render_device(self.ctx, ptr(d_rgba), ptr(d_rgb64), ptr(d_fate), s),
                     "grrt_render_device")
+
+    def render_rows_device(self, row0: int, row_step: int, n_rows: int, d_rgba=None, d_rgb64=None, d_fate=None,
+                           stream=None) -> None:
+        """Render image rows row0, row0 + row_step, ... (n_rows, full width) densely into device buffers."""
+        def ptr(x):
+            if x is None:
+                return None
+            return x if isinstance(x, int) else x.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_render_rows_device(self.ctx, row0, row_step, n_rows, ptr(d_rgba), ptr(d_rgb64),
+                                                    ptr(d_fate), s), "grrt_render_rows_device")
 
     def render_spectral_device(self, d_spec, width: int, height: int, d_fate=None, stream=None) -> None:
         def ptr(x):
@@ -579,3 +591,6 @@ def sweep_cameras(width: int = 256, height: int = 256, spins=(0.0, 0.5, 0.9, 0.9
 
 def cuda_available() -> bool:
     return bool(lib().grrt_cuda_available())
+
+
+from . import multi  # noqa: E402  (frame sharding across ranks)

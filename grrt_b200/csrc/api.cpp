@@ -106,6 +106,25 @@ extern "C" GRRT_EXPORT int grrt_render_tile(GRRTContext* ctx, float* buffer, int
     return ctx->render_rgb_to_host(tile, buffer, nullptr, nullptr);
 }
 
+extern "C" GRRT_EXPORT int grrt_render_rows_device(GRRTContext* ctx, int row0, int row_step, int n_rows,
+                                                   float* d_rgba, double* d_rgb64, unsigned int* d_fate,
+                                                   void* stream) {
+    if (!ctx) return -1;
+    if (row0 < 0 || row_step < 1 || n_rows < 1 ||
+        static_cast<long long>(row0) + static_cast<long long>(n_rows - 1) * row_step >= ctx->params.height) {
+        ctx->error = "grrt_render_rows_device: rows outside the image";
+        return -1;
+    }
+    DevTile tile;
+    tile.x0 = 0;
+    tile.y0 = row0;
+    tile.w = ctx->params.width;
+    tile.h = n_rows;
+    tile.out_pitch = ctx->params.width;
+    tile.row_step = row_step;
+    return ctx->render_rgb_device(tile, d_rgba, d_rgb64, d_fate, static_cast<cudaStream_t>(stream), true);
+}
+
 extern "C" GRRT_EXPORT void grrt_cancel(GRRTContext* ctx) {
     if (ctx) ctx->request_cancel();
 }

@@ -38,7 +38,7 @@ constexpr unsigned kMask = 0xffffffffu;
 __device__ __forceinline__ void sample_start(const DevScene& S, const DevTile& tile, unsigned q, int g2,
                                              Vec5<double>& y, double& pt, double& pph) {
     const int pix = static_cast<int>(q / g2), s = static_cast<int>(q % g2);
-    const int i = tile.x0 + pix % tile.w, j = tile.y0 + pix / tile.w;
+    const int i = tile.x0 + pix % tile.w, j = tile.y0 + (pix / tile.w) * tile.row_step;
     const int sy = s / S.grid, sx = s % S.grid;
     const double x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
     const double yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;

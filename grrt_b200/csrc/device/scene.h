@@ -90,11 +90,13 @@ struct DevScene {
     double mixed_margin = 0.05;
 };
 
-// Which pixels a launch covers: the rectangle [x0, x0+w) x [y0, y0+h) of the
-// image, written into an output of row pitch `out_pitch` pixels.
+// Which pixels a launch covers: columns [x0, x0+w) of the h image rows
+// y0, y0 + row_step, ..., y0 + (h-1) row_step (row_step 1: a rectangle),
+// written densely into an output of row pitch `out_pitch` pixels.
 struct DevTile {
     int x0 = 0, y0 = 0, w = 0, h = 0;
     int out_pitch = 0;
+    int row_step = 1;
 };
 
 // Batched form: one launch over many cameras. Items are camera images (or

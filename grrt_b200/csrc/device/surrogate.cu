@@ -501,7 +501,7 @@ cudaError_t launch_cast_weights(const float* params, __nv_bfloat16* const* wb, _
 __device__ __forceinline__ void sample_coords(const DevScene& S, const DevTile& tile, size_t q, double& x, double& yy) {
     const int g2 = S.grid * S.grid;
     const int pix = static_cast<int>(q / g2), s = static_cast<int>(q % g2);
-    const int i = tile.x0 + pix % tile.w, j = tile.y0 + pix / tile.w;
+    const int i = tile.x0 + pix % tile.w, j = tile.y0 + (pix / tile.w) * tile.row_step;
     const int sy = s / S.grid, sx = s % S.grid;
     x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
     yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;

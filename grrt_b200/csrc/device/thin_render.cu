@@ -136,7 +136,7 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
                     } else {
                         const int qx = static_cast<int>(q) % tile.w, qy = static_cast<int>(q) / tile.w;
                         px_i = tile.x0 + qx;
-                        px_j = tile.y0 + qy;
+                        px_j = tile.y0 + qy * tile.row_step;
                         px_out = static_cast<size_t>(qy) * tile.out_pitch + qx;
                         pix = static_cast<int>(q);
                         smp = 0;

@@ -87,7 +87,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
         }
         if (!live && pix >= 0) {
             const int qx = pix % tile.w, qy = pix / tile.w;
-            const int i = tile.x0 + qx, j = tile.y0 + qy;
+            const int i = tile.x0 + qx, j = tile.y0 + qy * tile.row_step;
             const int sy = smp / S.grid, sx = smp % S.grid;
             const double x = i + (sx + pixel_hash(i, j, smp, 0)) * S.cell;
             const double yy = j + (sy + pixel_hash(i, j, smp, 1)) * S.cell;

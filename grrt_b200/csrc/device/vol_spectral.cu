@@ -111,7 +111,7 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             const int pixel = kList ? pix / grid2 : pix;
             const int s = kList ? pix % grid2 : smp;
             const int qx = pixel % tile.w, qy = pixel / tile.w;
-            const int i = tile.x0 + qx, j = tile.y0 + qy;
+            const int i = tile.x0 + qx, j = tile.y0 + qy * tile.row_step;
             const int sy = s / S.grid, sx = s % S.grid;
             const double x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
             const double yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;
@@ -499,7 +499,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
             } else {
                 q = k;
                 const int pixel = static_cast<int>(q / g2), s = static_cast<int>(q % g2);
-                const int i = tile.x0 + pixel % tile.w, j = tile.y0 + pixel / tile.w;
+                const int i = tile.x0 + pixel % tile.w, j = tile.y0 + (pixel / tile.w) * tile.row_step;
                 const int sy = s / S.grid, sx = s % S.grid;
                 const double x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
                 const double yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;

@@ -74,6 +74,13 @@ GRRT_EXPORT int grrt_get_phase_ms(GRRTContext* ctx, double* out, int capacity);
 GRRT_EXPORT int grrt_render_device(GRRTContext* ctx, float* d_rgba, double* d_rgb64,
                                    unsigned int* d_fate, void* stream);
 
+/* The same for the n_rows image rows row0, row0 + row_step, ... at full width,
+ * written densely (output row k = image row row0 + k * row_step): a rank's
+ * share of a frame split across GPUs by interleaved rows. Each pixel is
+ * computed exactly as in the full render. -1 when a row lies outside the image. */
+GRRT_EXPORT int grrt_render_rows_device(GRRTContext* ctx, int row0, int row_step, int n_rows, float* d_rgba,
+                                        double* d_rgb64, unsigned int* d_fate, void* stream);
+
 /* Spectral render into device memory (Renderer::render_spectral,
  * src/renderer.cpp:84-138): d_spec double[width*height*bins]. */
 GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double* d_spec, int width, int height,
