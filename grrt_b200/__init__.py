@@ -139,7 +139,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_surrogate_render_device": (C.c_int, [vp, vp, vp, vp, vp, vp]),
         "grrt_surrogate_render": (C.c_int, [vp, vp, P(C.c_float)]),
         "grrt_surrogate_last_exact": (C.c_int, [vp, P(C.c_longlong), P(C.c_longlong)]),
-        "grrt_surrogate_last_counts": (C.c_int, [vp, P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]),
+        "grrt_surrogate_last_counts": (C.c_int, [vp, P(C.c_longlong), P(C.c_longlong), P(C.c_longlong),
+                                                 P(C.c_longlong)]),
         "grrt_surrogate_save": (C.c_int, [vp, C.c_char_p]),
         "grrt_surrogate_load": (C.c_int, [vp, C.c_char_p]),
         "grrt_surrogate_gemm_bf16": (C.c_int, [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp,
@@ -558,11 +559,12 @@ class Surrogate:
         return e.value, n.value
 
     def last_counts(self) -> dict:
-        """Samples of the last render: re-traced exactly, sent to the FP32 speculation, total."""
-        e, sp, n = C.c_longlong(), C.c_longlong(), C.c_longlong()
-        self._check(self._L.grrt_surrogate_last_counts(self.s, C.byref(e), C.byref(sp), C.byref(n)),
+        """Samples of the last render: re-traced exactly, sent to the FP32 speculation,
+        evaluated by the network (the rest settled in closed form), total."""
+        e, sp, nw, n = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._check(self._L.grrt_surrogate_last_counts(self.s, C.byref(e), C.byref(sp), C.byref(nw), C.byref(n)),
                     "grrt_surrogate_last_counts")
-        return {"exact": e.value, "speculated": sp.value, "samples": n.value}
+        return {"exact": e.value, "speculated": sp.value, "network": nw.value, "samples": n.value}
 
     def save(self, path: str) -> None:
         self._check(self._L.grrt_surrogate_save(self.s, path.encode()), "grrt_surrogate_save")

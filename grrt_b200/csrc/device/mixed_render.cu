@@ -27,6 +27,7 @@
 #include "mixed_spec.cuh"
 #include "render_launch.h"
 #include "shading.cuh"
+#include "surrogate_geom.cuh"
 
 namespace grrt_b200 {
 
@@ -157,6 +158,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
     Vec5<double> y;
     Vec5<float> k1;  // FP32 f(y), kept from the previous attempt when k1_ok
     bool k1_ok = false;
+    bool settled = false;  // black sky, never reaches the disk: final without a trace
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0;
     mixed::Tracker trk;
@@ -181,6 +183,19 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                     trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.fp32_r_min);
                 else
                     trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near);
+                // Black sky: a ray whose smallest radius (closed form, from its
+                // constants of motion) lies outside the disk, r_near and every
+                // photon orbit escapes with colour 0 and no crossing.
+                settled = false;
+                if (!S.stars_on && (kBatch || !mb.spec_list)) {
+                    const double p[4] = {pt, y.pr, y.pth, pph};
+                    const double m = kBatch ? S.mixed_margin : mb.margin;
+                    const double r_near = kBatch ? S.fp32_r_min : mb.r_near;
+                    const double r_gate =
+                        fmax(fmax(mixed::kEscapeRMin * S.M, r_near), S.disk_on ? S.r_out + 2.0 * m : 0.0);
+                    settled = surr::camera_ray_min_radius(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p) >
+                              r_gate;
+                }
                 live = true;
             }
         }
@@ -189,6 +204,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
         bool retrace = false;
         Vec5<float> k7;
         if (live && retry == 0) term = start_test(S, step, y.r);
+        if (live && term < 0 && settled) term = kTermEscaped;
         if (live && term < 0) {
             if (!k1_ok) {
                 k1 = mixed_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y);

@@ -95,8 +95,12 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-mlp_fused_kernel(const __grid_constant__ FusedMaps maps, const float* __restrict__ X, long long n,
-                 const float* __restrict__ params, float* __restrict__ out, int* err) {
+mlp_fused_kernel(const __grid_constant__ FusedMaps maps, const float* __restrict__ X, long long n_cap,
+                 const unsigned* __restrict__ n_dev, const float* __restrict__ params, float* __restrict__ out,
+                 int* err) {
+    // the row count: n_cap, or the device count a previous kernel wrote (at most n_cap)
+    const long long n = n_dev ? (static_cast<long long>(*n_dev) < n_cap ? static_cast<long long>(*n_dev) : n_cap)
+                              : n_cap;
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = sm100::smem_u32(smem_raw);
     unsigned char* act = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
@@ -297,7 +301,8 @@ bool weight_map(CUtensorMap* m, const __nv_bfloat16* w, int rows) {
 size_t mlp_fused_smem_bytes() { return 1024 + kActBytes + kStages * kStageBytes + sizeof(FusedSmem); }
 
 cudaError_t launch_mlp_fused(const float* X, long long n, const float* params, __nv_bfloat16* const* wb,
-                             const __nv_bfloat16* w5b, float* out, int* d_err, cudaStream_t s) {
+                             const __nv_bfloat16* w5b, float* out, int* d_err, cudaStream_t s,
+                             const unsigned* d_n) {
     if (n <= 0) return cudaSuccess;
     if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(out) & 15)) return cudaErrorInvalidValue;
     FusedMaps maps;
@@ -317,7 +322,7 @@ cudaError_t launch_mlp_fused(const float* X, long long n, const float* params, _
     if (attr != cudaSuccess) return attr;
     const long long tiles = (n + kRows - 1) / kRows;
     const int grid = static_cast<int>(tiles < sms ? tiles : sms);
-    mlp_fused_kernel<<<grid, kThreads, mlp_fused_smem_bytes(), s>>>(maps, X, n, params, out, d_err);
+    mlp_fused_kernel<<<grid, kThreads, mlp_fused_smem_bytes(), s>>>(maps, X, n, d_n, params, out, d_err);
     return cudaGetLastError();
 }
 

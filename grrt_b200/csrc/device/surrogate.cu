@@ -508,26 +508,61 @@ __device__ __forceinline__ void sample_coords(const DevScene& S, const DevTile& 
 }
 
 __global__ void prepare_kernel(const __grid_constant__ DevScene S, const DevTile tile, size_t q0, size_t nq,
-                               float* __restrict__ X, SampleAux* __restrict__ aux) {
+                               double settle_radius, float* __restrict__ X, SampleAux* __restrict__ aux,
+                               unsigned* __restrict__ count, unsigned* __restrict__ total, DevMixedBuffers mb,
+                               DevStats* stats) {
+    // whole warps stay together for the ballots
     const size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    if (k >= nq) return;
-    double x, yy, p[4], alpha, beta;
-    sample_coords(S, tile, q0 + k, x, yy);
-    pixel_ray(S, x, yy, p, alpha, beta);
+    const int lane = threadIdx.x & 31;
+    bool keep = false, settled = false;
+    double p[4] = {0, 0, 0, 0}, alpha = 0, beta = 0;
+    const unsigned q = static_cast<unsigned>(q0 + k);
+    if (k < nq) {
+        double x, yy;
+        sample_coords(S, tile, q0 + k, x, yy);
+        pixel_ray(S, x, yy, p, alpha, beta);
+        // black sky: never near the disk, the hole or a photon orbit (closed
+        // form): colour 0 and escaped, as the FP64 method gives it
+        settled = settle_radius > 0.0 &&
+                  camera_ray_min_radius(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p) > settle_radius;
+        keep = !settled;
+        if (settled) {
+            mb.sample_rgb[3 * static_cast<size_t>(q) + 0] = 0.0;
+            mb.sample_rgb[3 * static_cast<size_t>(q) + 1] = 0.0;
+            mb.sample_rgb[3 * static_cast<size_t>(q) + 2] = 0.0;
+            mb.sample_fate[q] = static_cast<unsigned>(kTermEscaped);
+        }
+    }
+    const unsigned m = __ballot_sync(kMask, keep);
+    const unsigned ns = __popc(__ballot_sync(kMask, settled));
+    if (lane == 0 && ns) atomicAdd(&stats->rays, static_cast<unsigned long long>(ns));
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) {
+        base = atomicAdd(count, static_cast<unsigned>(__popc(m)));
+        atomicAdd(total, static_cast<unsigned>(__popc(m)));
+    }
+    base = __shfl_sync(kMask, base, leader);
+    if (!keep) return;
+    const unsigned j = base + __popc(m & ((1u << lane) - 1u));
     float in[4];
     encode_inputs(alpha, beta, S.a, S.cam_pos[2], in);
-    *reinterpret_cast<float4*>(X + 4 * k) = make_float4(in[0], in[1], in[2], in[3]);
+    *reinterpret_cast<float4*>(X + 4 * static_cast<size_t>(j)) = make_float4(in[0], in[1], in[2], in[3]);
     SampleAux a;
     a.pt = p[0];
     a.pph = p[3];
     ray_margins(S, p, a.capture_margin, a.graze_margin);
-    aux[k] = a;
+    a.q = q;
+    aux[j] = a;
 }
 
-cudaError_t launch_prepare(const DevScene& S, const DevTile& tile, size_t q0, size_t nq, float* X, SampleAux* aux,
-                           cudaStream_t s) {
+cudaError_t launch_prepare(const DevScene& S, const DevTile& tile, size_t q0, size_t nq, double settle_radius,
+                           float* X, SampleAux* aux, unsigned* count, unsigned* total, const DevMixedBuffers& mb,
+                           DevStats* stats, cudaStream_t s) {
     if (nq == 0) return cudaSuccess;
-    prepare_kernel<<<static_cast<unsigned>((nq + 127) / 128), 128, 0, s>>>(S, tile, q0, nq, X, aux);
+    prepare_kernel<<<static_cast<unsigned>((nq + 127) / 128), 128, 0, s>>>(S, tile, q0, nq, settle_radius, X, aux,
+                                                                          count, total, mb, stats);
     return cudaGetLastError();
 }
 
@@ -551,16 +586,18 @@ __device__ __forceinline__ void append(bool want, unsigned q, unsigned* count, u
     if (want) list[base + __popc(m & ((1u << lane) - 1u))] = q;
 }
 
-__global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile tile, size_t q0, size_t nq,
-                             const float* __restrict__ O, const SampleAux* __restrict__ aux, RenderBands bands,
-                             DevMixedBuffers mb, DevStats* stats) {
+__global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile tile, const unsigned* count,
+                             size_t cap, const float* __restrict__ O, const SampleAux* __restrict__ aux,
+                             RenderBands bands, DevMixedBuffers mb, DevStats* stats) {
     // whole warps stay together for the ballots in append
     const size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    const size_t nq = *count < cap ? *count : cap;
     bool exact = false;    // colour depends on the FP64 steps: re-trace
     bool uncertain = false;  // the network cannot rule out the disk: FP32 speculation decides
-    const unsigned q = static_cast<unsigned>(q0 + k);
+    unsigned q = 0;
     if (k < nq) {
         const SampleAux a = aux[k];
+        q = a.q;
         const float* o = O + k * kOutPad;
         if (fabsf(a.capture_margin) < bands.capture || a.graze_margin < bands.graze) exact = true;
         const bool captured = a.capture_margin > 0.0f;
@@ -640,11 +677,13 @@ __global__ void shade_kernel(const __grid_constant__ DevScene S, const DevTile t
     if ((threadIdx.x & 31) == 0 && live) atomicAdd(&stats->rays, static_cast<unsigned long long>(__popc(live)));
 }
 
-cudaError_t launch_shade(const DevScene& S, const DevTile& tile, size_t q0, size_t nq, const float* O,
+cudaError_t launch_shade(const DevScene& S, const DevTile& tile, const unsigned* count, size_t cap, const float* O,
                          const SampleAux* aux, const RenderBands& bands, const DevMixedBuffers& mb, DevStats* stats,
                          cudaStream_t s) {
+    const size_t nq = cap;
     if (nq == 0) return cudaSuccess;
-    shade_kernel<<<static_cast<unsigned>((nq + 127) / 128), 128, 0, s>>>(S, tile, q0, nq, O, aux, bands, mb, stats);
+    shade_kernel<<<static_cast<unsigned>((nq + 127) / 128), 128, 0, s>>>(S, tile, count, cap, O, aux, bands, mb,
+                                                                        stats);
     return cudaGetLastError();
 }
 

@@ -101,10 +101,18 @@ struct RenderBands {
 struct SampleAux {
     double pt, pph;
     float capture_margin, graze_margin;
+    unsigned q;  // the sample
 };
-cudaError_t launch_prepare(const DevScene& S, const DevTile& tile, size_t q0, size_t nq, float* X, SampleAux* aux,
-                           cudaStream_t s);
-cudaError_t launch_shade(const DevScene& S, const DevTile& tile, size_t q0, size_t nq, const float* O,
+// Samples q0 .. q0 + nq - 1 of the tile. With settle_radius > 0 (a black
+// sky), a sample whose closed-form smallest radius exceeds it is final at
+// once (colour 0, escaped, written to mb) and skips the network; the others
+// are appended to X / aux, *count of them (zeroed by the caller), and added
+// to *total (the render's network samples).
+cudaError_t launch_prepare(const DevScene& S, const DevTile& tile, size_t q0, size_t nq, double settle_radius,
+                           float* X, SampleAux* aux, unsigned* count, unsigned* total, const DevMixedBuffers& mb,
+                           DevStats* stats, cudaStream_t s);
+// Shades the *count prepared samples (at most cap) from the network outputs O.
+cudaError_t launch_shade(const DevScene& S, const DevTile& tile, const unsigned* count, size_t cap, const float* O,
                          const SampleAux* aux, const RenderBands& bands, const DevMixedBuffers& mb, DevStats* stats,
                          cudaStream_t s);
 

@@ -93,6 +93,44 @@ GRRT_HD double capture_margin(double M, double a, const RayConstants& k, double 
     return v < best ? v : best;
 }
 
+// Smallest radius of a ray that starts at r_cam moving inward: its outermost
+// radial turning point (largest root of R below r_cam), or r_h when it falls
+// in. R / (E^2 r^4) is scanned on a geometric grid from r_cam inward and the
+// first sign change is bisected; the result is taken on the forbidden side,
+// so it never exceeds the root. A forbidden interval narrower than the grid
+// spacing is missed and the ray counts as falling in (a smaller radius).
+GRRT_HD double turning_radius(double M, double a, const RayConstants& k, double r_h, double r_cam) {
+    constexpr int kN = 96;
+    const double lo = r_h * (1.0 + 1e-9);
+    const double q = pow(r_cam / lo, 1.0 / (kN - 1));
+    double r_prev = r_cam;
+    for (int i = 1; i < kN; ++i) {
+        const double r = (i == kN - 1) ? lo : r_prev / q;
+        if (scaled_potential(M, a, k, r) < 0.0) {
+            double x0 = r, x1 = r_prev;
+            for (int it = 0; it < 60; ++it) {
+                const double xm = 0.5 * (x0 + x1);
+                if (scaled_potential(M, a, k, xm) < 0.0)
+                    x0 = xm;
+                else
+                    x1 = xm;
+            }
+            return x0;
+        }
+        r_prev = r;
+    }
+    return r_h;
+}
+
+// Smallest radius a camera ray (covariant momentum p at the camera, r_cam,
+// theta_cam) ever reaches: r_cam for an outgoing ray (it only moves out:
+// every photon orbit lies far inside the camera radius), else turning_radius.
+GRRT_HD double camera_ray_min_radius(double M, double a, double r_h, double r_cam, double theta_cam,
+                                     const double p[4]) {
+    if (p[1] >= 0.0) return r_cam;
+    return turning_radius(M, a, constants(a, theta_cam, p), r_h, r_cam);
+}
+
 // Distance (in mu = cos theta) of the ray's theta turning point from the
 // equator: mu_+ when Q >= 0 (the ray crosses the plane and turns at +-mu_+),
 // mu_- when Q < 0 (it stays in one hemisphere between mu_- and mu_+).

@@ -412,40 +412,11 @@ struct ReachRay {
     bool far = false;     // never inside r <= R: no step test needed
 };
 
-// Smallest radius of a ray starting at r_cam moving inward: its outermost
-// radial turning point (largest root of R(r) below r_cam), or r_h when it
-// falls in. R / (E^2 r^4) is scanned on a geometric grid from r_cam inward;
-// the first sign change is bisected (the result is taken on the forbidden
-// side, so it never exceeds the root). A forbidden interval narrower than
-// the grid spacing is missed and the ray counts as falling in (smaller r).
-__device__ double turning_radius(double M, double a, const surr::RayConstants& k, double r_h, double r_cam) {
-    constexpr int kN = 96;
-    const double lo = r_h * (1.0 + 1e-9);
-    const double q = pow(r_cam / lo, 1.0 / (kN - 1));
-    double r_prev = r_cam;
-    for (int i = 1; i < kN; ++i) {
-        const double r = (i == kN - 1) ? lo : r_prev / q;
-        if (surr::scaled_potential(M, a, k, r) < 0.0) {
-            double x0 = r, x1 = r_prev;
-            for (int it = 0; it < 60; ++it) {
-                const double xm = 0.5 * (x0 + x1);
-                if (surr::scaled_potential(M, a, k, xm) < 0.0)
-                    x0 = xm;
-                else
-                    x1 = xm;
-            }
-            return x0;
-        }
-        r_prev = r;
-    }
-    return r_h;
-}
-
 __device__ ReachRay reach_ray(const DevScene& S, const VolReach& v, const double p[4]) {
     ReachRay rr;
     const double r_cam = S.cam_pos[1];
     const surr::RayConstants kc = surr::constants(S.a, S.cam_pos[2], p);
-    rr.r_turn = (p[1] >= 0.0) ? r_cam : turning_radius(S.M, S.a, kc, S.r_stop - 0.01, r_cam);
+    rr.r_turn = (p[1] >= 0.0) ? r_cam : surr::turning_radius(S.M, S.a, kc, S.r_stop - 0.01, r_cam);
     rr.mu_lo = (kc.Q < 0.0) ? surr::graze_margin(S.a, kc) : 0.0;
     rr.far = rr.r_turn - (v.margin + 1e-3 * v.R) > v.R;
     return rr;
@@ -524,6 +495,9 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
             if (step >= S.max_steps) term = kTermMaxSteps;
             else if (y.r < S.r_stop) term = kTermHorizon;
             else if (y.r > S.r_escape) term = kTermEscaped;
+            // never inside R: a turning point there, so it escapes, and the
+            // plain stepping it gets has zero intensity; nothing to trace
+            else if (step == 0 && rr.far) term = kTermEscaped;
         }
         if (live && term < 0) {
             if (!k1_ok) {

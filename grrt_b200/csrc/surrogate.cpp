@@ -89,6 +89,7 @@ struct GRRTSurrogate {
     size_t inf_chunk = 0;
     float *iX = nullptr, *iO = nullptr;
     SampleAux* iaux = nullptr;
+    unsigned* icount = nullptr;  // samples of the chunk that go through the network
     static constexpr size_t kChunk = size_t(1) << 22;
 
     RenderBands bands;
@@ -97,8 +98,9 @@ struct GRRTSurrogate {
     float last_loss = NAN;
     LossWeights weights;
     size_t last_render_samples = 0;
-    const unsigned* last_retrace_count = nullptr;
-    const unsigned* last_spec_count = nullptr;
+    // counts of the last render, copied into the surrogate's own buffer
+    // (icount[1..3]: network, exact, speculated) so they outlive the context
+    bool have_counts = false;
 
     ~GRRTSurrogate() {
         if (device >= 0) cudaSetDevice(device);
@@ -160,7 +162,9 @@ struct GRRTSurrogate {
         dfree(iX);
         dfree(iO);
         dfree(iaux);
+        dfree(icount);
         inf_chunk = 0;
+        have_counts = false;
     }
 
     bool init(unsigned seed) {
@@ -465,7 +469,8 @@ struct GRRTSurrogate {
     bool ensure_inference(size_t chunk) {
         if (inf_chunk >= chunk) return true;
         free_inference();
-        if (!dalloc(&iX, chunk * kIn) || !dalloc(&iO, chunk * kOutPad) || !dalloc(&iaux, chunk)) {
+        if (!dalloc(&iX, chunk * kIn) || !dalloc(&iO, chunk * kOutPad) || !dalloc(&iaux, chunk) ||
+            !dalloc(&icount, 64)) {
             free_inference();
             return !fail_msg("cudaMalloc(inference workspace) failed");
         }
@@ -473,9 +478,10 @@ struct GRRTSurrogate {
         return true;
     }
 
-    // O[n x 16] = network(X[n x 4]): the fused tensor-core kernel
-    bool enqueue_forward(const float* X, size_t n, float* out) {
-        return !fail(launch_mlp_fused(X, static_cast<long long>(n), d_params, d_wb, d_w5b, out, d_err, stream),
+    // O[n x 16] = network(X[n x 4]): the fused tensor-core kernel (rows
+    // min(n, *d_n) when a device count is given)
+    bool enqueue_forward(const float* X, size_t n, float* out, const unsigned* d_n = nullptr) {
+        return !fail(launch_mlp_fused(X, static_cast<long long>(n), d_params, d_wb, d_w5b, out, d_err, stream, d_n),
                      "fused network");
     }
 
@@ -512,12 +518,24 @@ struct GRRTSurrogate {
         if (fail(cudaMemsetAsync(ctx->d_stats, 0, sizeof(DevStats), stream), "memset") ||
             fail(cudaMemsetAsync(ctx->d_mixed_scratch, 0, 1024, stream), "memset"))
             return false;
-        // network and shading, chunk by chunk
+        // On a black sky a sample whose closed-form smallest radius lies
+        // outside the disk, r_near and every photon orbit is settled by the
+        // prepare pass (colour 0, escaped) and skips the network.
+        const double settle_radius =
+            S.stars_on ? 0.0
+                       : std::max(std::max(5.0 * S.M, mb.r_near), S.disk_on ? S.r_out + 2.0 * mb.margin : 0.0);
+        // network and shading, chunk by chunk (icount[1]: the render's network samples)
+        if (fail(cudaMemsetAsync(icount + 1, 0, sizeof(unsigned), stream), "memset")) return false;
         for (size_t q0 = 0; q0 < n; q0 += kChunk) {
             const size_t nq = std::min(kChunk, n - q0);
-            if (fail(launch_prepare(S, tile, q0, nq, iX, iaux, stream), "prepare")) return false;
-            if (!enqueue_forward(iX, nq, iO)) return false;
-            if (fail(launch_shade(S, tile, q0, nq, iO, iaux, bands, mb, ctx->d_stats, stream), "shade")) return false;
+            if (fail(cudaMemsetAsync(icount, 0, sizeof(unsigned), stream), "memset") ||
+                fail(launch_prepare(S, tile, q0, nq, settle_radius, iX, iaux, icount, icount + 1, mb, ctx->d_stats,
+                                    stream),
+                     "prepare"))
+                return false;
+            if (!enqueue_forward(iX, nq, iO, icount)) return false;
+            if (fail(launch_shade(S, tile, icount, nq, iO, iaux, bands, mb, ctx->d_stats, stream), "shade"))
+                return false;
         }
         cudaEventRecord(ctx->ev_phase[1], stream);
         // the uncertain samples: FP32 speculation (and its star pass) settles the
@@ -534,6 +552,11 @@ struct GRRTSurrogate {
         out.rgb64 = d_rgb64;
         out.fate = d_fate;
         if (fail(launch_mixed_resolve(S, tile, mb, out, ctx->d_stats, stream), "resolve")) return false;
+        if (fail(cudaMemcpyAsync(icount + 2, mb.retrace_count, sizeof(unsigned), cudaMemcpyDeviceToDevice, stream),
+                 "counts") ||
+            fail(cudaMemcpyAsync(icount + 3, mb.spec_count, sizeof(unsigned), cudaMemcpyDeviceToDevice, stream),
+                 "counts"))
+            return false;
         cudaEventRecord(ctx->ev_phase[4], stream);
         cudaEventRecord(ctx->ev1, stream);
         ctx->n_phases = kMixedPhases;
@@ -544,8 +567,7 @@ struct GRRTSurrogate {
         cudaStreamWaitEvent(s, e_out, 0);
         cudaEventDestroy(e_out);
         last_render_samples = n;
-        last_retrace_count = mb.retrace_count;
-        last_spec_count = mb.spec_count;
+        have_counts = true;
         return true;
     }
 
@@ -863,24 +885,23 @@ extern "C" GRRT_EXPORT int grrt_surrogate_load(GRRTSurrogate* s, const char* pat
 }
 
 extern "C" GRRT_EXPORT int grrt_surrogate_last_counts(const GRRTSurrogate* s, long long* exact,
-                                                      long long* speculated, long long* samples) {
+                                                      long long* speculated, long long* network, long long* samples) {
     if (!s || !exact || !samples) return -1;
-    unsigned h[2] = {0, 0};
-    const unsigned* src[2] = {s->last_retrace_count, s->last_spec_count};
-    for (int k = 0; k < 2; ++k) {
-        if (!src[k]) continue;
+    unsigned h[3] = {0, 0, 0};  // network, exact, speculated
+    if (s->have_counts) {
         cudaSetDevice(s->device);
-        if (s->copy(&h[k], src[k], sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (s->copy(h, s->icount + 1, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) {
             cudaGetLastError();
             return -1;
         }
     }
-    *exact = h[0];
-    if (speculated) *speculated = h[1];
+    *exact = h[1];
+    if (speculated) *speculated = h[2];
+    if (network) *network = h[0];
     *samples = static_cast<long long>(s->last_render_samples);
     return 0;
 }
 
 extern "C" GRRT_EXPORT int grrt_surrogate_last_exact(const GRRTSurrogate* s, long long* exact, long long* samples) {
-    return grrt_surrogate_last_counts(s, exact, nullptr, samples);
+    return grrt_surrogate_last_counts(s, exact, nullptr, nullptr, samples);
 }

@@ -116,11 +116,13 @@ GRRT_EXPORT int grrt_surrogate_gradients(GRRTSurrogate* s, const float* h_in, co
 GRRT_EXPORT int grrt_surrogate_render_device(GRRTSurrogate* s, GRRTContext* ctx, float* d_rgba, double* d_rgb64,
                                              unsigned int* d_fate, void* stream);
 GRRT_EXPORT int grrt_surrogate_render(GRRTSurrogate* s, GRRTContext* ctx, float* framebuffer);
-/* Samples re-traced exactly and samples in the last render (the context must still exist). */
+/* Samples re-traced exactly and samples in the last render. */
 GRRT_EXPORT int grrt_surrogate_last_exact(const GRRTSurrogate* s, long long* exact, long long* samples);
-/* The same, plus the samples sent to the FP32 speculation (speculated may be NULL). */
+/* The same, plus the samples sent to the FP32 speculation and the samples the
+ * network evaluated (the rest were settled in closed form on a black sky);
+ * speculated and network may be NULL. */
 GRRT_EXPORT int grrt_surrogate_last_counts(const GRRTSurrogate* s, long long* exact, long long* speculated,
-                                           long long* samples);
+                                           long long* network, long long* samples);
 
 GRRT_EXPORT int grrt_surrogate_save(const GRRTSurrogate* s, const char* path);
 GRRT_EXPORT int grrt_surrogate_load(GRRTSurrogate* s, const char* path);

@@ -50,6 +50,16 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
     trk.reset(disk_on, sc[7], sc[8], sc[9], sc[10]);
     Vec5<float> k7{};
     *term_out = -1;
+    // black sky: a ray whose closed-form smallest radius lies outside the disk,
+    // r_near and every photon orbit is final at once (as the kernel)
+    if (!stars_on) {
+        const double p[4] = {y8[4], y8[5], y8[6], y8[7]};
+        const double r_gate = fmax(fmax(mixed::kEscapeRMin * M, sc[10]), disk_on ? sc[8] + 2.0 * sc[9] : 0.0);
+        if (surr::camera_ray_min_radius(M, a, r_stop - 0.01, y8[1], y8[2], p) > r_gate) {
+            *term_out = kTermEscaped;
+            return 0;
+        }
+    }
     while (true) {
         if (retry == 0) {
             if (step >= max_steps) { *term_out = kTermMaxSteps; return 1; }
