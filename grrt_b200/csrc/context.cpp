@@ -289,7 +289,7 @@ bool GRRTContext::ensure_device() {
 
 DevScene GRRTContext::scene_for_launch() const {
     DevScene S = dev;
-    S.fp32_r_min = mixed_r_factor * r_horizon;
+    S.r_near_mixed = mixed_r_factor * r_horizon;
     S.tol_fp32 = tol_fp32;
     S.mixed_margin = mixed_margin;
     return S;

@@ -3,7 +3,7 @@
 // are in mixed_spec.cuh).
 //
 //   speculate: every sample is integrated with FP32 right-hand sides and FP64
-//     state (mixed_attempt_impl) against a relaxed tolerance. A sample that
+//     state (mixed_attempt_k1) against a relaxed tolerance. A sample that
 //     needs the FP64 step sequence is queued for the re-trace and dropped; a
 //     horizon sample is final (colour 0); an escape stores its sky arc for the
 //     star pass.
@@ -180,7 +180,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                 step = 0;
                 k1_ok = false;
                 if (kBatch)
-                    trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.fp32_r_min);
+                    trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.r_near_mixed);
                 else
                     trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near);
                 // Black sky: a ray whose smallest radius (closed form, from its
@@ -190,7 +190,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                 if (!S.stars_on && (kBatch || !mb.spec_list)) {
                     const double p[4] = {pt, y.pr, y.pth, pph};
                     const double m = kBatch ? S.mixed_margin : mb.margin;
-                    const double r_near = kBatch ? S.fp32_r_min : mb.r_near;
+                    const double r_near = kBatch ? S.r_near_mixed : mb.r_near;
                     const double r_gate =
                         fmax(fmax(mixed::kEscapeRMin * S.M, r_near), S.disk_on ? S.r_out + 2.0 * m : 0.0);
                     settled = surr::camera_ray_min_radius(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p) >
@@ -227,7 +227,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                 // black sky: an escape is final as soon as it is certain
                 if (term < 0 && !S.stars_on) {
                     const double m = kBatch ? S.mixed_margin : mb.margin;
-                    const double r_near = kBatch ? S.fp32_r_min : mb.r_near;
+                    const double r_near = kBatch ? S.r_near_mixed : mb.r_near;
                     const double r_min = fmax(fmax(mixed::kEscapeRMin * S.M, r_near),
                                               S.disk_on ? S.r_out + 2.0 * m : 0.0);
                     if (mixed::certain_escape(y, r_min, step, S.max_steps)) term = kTermEscaped;

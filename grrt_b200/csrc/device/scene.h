@@ -80,12 +80,12 @@ struct DevScene {
     int vol_on = 0;
     DevVolume vol;
 
-    // mixed-precision forms. Volumetric: outer steps starting at r >
-    // fp32_r_min use FP32 right-hand sides, controlled against tol_fp32.
-    // Thin disk: the FP32 speculation runs against tol_fp32 and re-traces in
-    // FP64 the escapes that came inside fp32_r_min and the samples whose
-    // crossings fall within mixed_margin of a disk edge.
-    double fp32_r_min = 0;
+    // mixed forms (speculative FP32 pass, then FP64 re-trace): the FP32
+    // tolerance; r_near_mixed = r_factor x r_horizon, inside which a
+    // near-critical sweep sends a sample to the re-trace (and beyond which,
+    // on a black sky, a certain escape is final); mixed_margin, the disk-radius
+    // margin of the re-trace test
+    double r_near_mixed = 0;
     double tol_fp32 = 1e-6;
     double mixed_margin = 0.05;
 };

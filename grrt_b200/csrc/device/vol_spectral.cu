@@ -483,7 +483,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
-                trk.reset(false, 0.0, 0.0, 0.0, S.fp32_r_min);
+                trk.reset(false, 0.0, 0.0, 0.0, S.r_near_mixed);
                 k1_ok = false;
                 live = true;
             }
@@ -521,7 +521,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
                 if (retrace)
                     term = kTermMaxSteps;
                 else if (mixed::certain_escape(y,
-                                               fmax(fmax(mixed::kEscapeRMin * S.M, S.fp32_r_min),
+                                               fmax(fmax(mixed::kEscapeRMin * S.M, S.r_near_mixed),
                                                     reach.R + 2.0 * reach.margin + 2e-3 * y.r),
                                                step, S.max_steps))
                     term = kTermEscaped;  // spectra carry no sky: the escape is final once certain
