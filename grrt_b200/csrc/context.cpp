@@ -329,8 +329,9 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     out.fate = d_fate;
     const DevScene S = scene_for_launch();
     const bool mixed_thin = !vol && form == GRRT_FORM_MIXED;
+    const bool mixed_vol = vol && form == GRRT_FORM_MIXED;
     size_t mixed_bytes = 0;
-    if (mixed_thin) {
+    if (mixed_thin || mixed_vol) {
         mixed_bytes = mixed_scratch_bytes(tile, S.grid * S.grid);
         if (mixed_bytes > d_mixed_scratch_bytes) {
             cudaFree(d_mixed_scratch);
@@ -343,15 +344,18 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     n_phases = 0;
     cudaEventRecord(ev0, s);
     cudaError_t e;
-    if (vol)
-        e = launch_volume_rgb(S, tile, out, res, form, s);
+    if (mixed_vol)
+        e = launch_volume_rgb_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, vol_reach_z, ev_phase,
+                                    s);
+    else if (vol)
+        e = launch_volume_rgb(S, tile, out, res, s);
     else if (mixed_thin)
         e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
                               mixed_r_factor * r_horizon, ev_phase, s);
     else
         e = launch_thin(S, tile, out, res, s);
     cudaEventRecord(ev1, s);
-    n_phases = mixed_thin ? kMixedPhases : 0;
+    n_phases = (mixed_thin || mixed_vol) ? kMixedPhases : 0;
     if (fail_cuda(e, "render launch")) return -1;
     return 0;
 }

@@ -54,8 +54,17 @@ size_t volume_spectral_scratch_elems(int nb);
 cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                         const LaunchResources& res, cudaStream_t stream);
 
+// Volumetric RGB render, FP64 form; and its mixed form (FP32 speculation with
+// the thin form's star pass, FP64 re-trace, resolve: scratch of
+// mixed_scratch_bytes, phase_events NULL or kMixedPhases + 1 events).
 cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                              const LaunchResources& res, int form, cudaStream_t stream);
+                              const LaunchResources& res, cudaStream_t stream);
+cudaError_t launch_volume_rgb_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                                    const LaunchResources& res, void* scratch, size_t scratch_bytes, double reach_z,
+                                    cudaEvent_t* phase_events, cudaStream_t stream);
+// The mixed form's FP64 re-trace of mb.retrace_list (mb.queue2 zeroed).
+cudaError_t launch_volume_rgb_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                                      DevStats* stats, const volatile int* cancel, cudaStream_t stream);
 
 // Spectral render, FP64 form (vol_spectral.cu: warp-cooperative transfer).
 constexpr int kVolSpectralThreads = 128;

@@ -8,7 +8,8 @@
 // Same persistent execution model as the thin-disk kernel: a lane owns one
 // pixel, one loop iteration advances each live ray by one DP45 attempt (outer
 // phase) or one RK4 march step (march phase); the three channels' transfer
-// state sits in registers. Both precision forms run the FP64 method here.
+// state sits in registers. The list instantiation is the FP64 re-trace of the
+// mixed form (its speculation is in vol_spectral.cu).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -36,14 +37,21 @@ __device__ __forceinline__ double rgb_nu(int ch) {
 }  // namespace
 
 // Three channels in registers; the march ends when all T < 1e-6.
+// kList = false: work item = pixel of the tile, spp samples summed into the
+// outputs. kList = true (the mixed form's re-trace): work item k = sample
+// list[k] (pixel * grid^2 + s); out_d[3 q ..] receives the sample's colour and
+// out_fate[q] its fate; rays and terminations are counted by the mixed form's
+// other passes.
+template <bool kList>
 __global__ void __launch_bounds__(kVolThreads)
 vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
                   double* __restrict__ out_d, uint32_t* __restrict__ out_fate, unsigned int* __restrict__ queue,
-                  DevStats* __restrict__ stats, const volatile int* __restrict__ cancel) {
+                  DevStats* __restrict__ stats, const volatile int* __restrict__ cancel,
+                  const unsigned* __restrict__ list, const unsigned* __restrict__ list_count) {
     const DevVolume& V = S.vol;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
+    const unsigned total = kList ? *list_count : static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
     const int grid2 = S.grid * S.grid;
 
     VolCounters cnt;
@@ -77,7 +85,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             if (want) {
                 const unsigned q = base + __popc(want_mask & lt_mask);
                 if (q < total) {
-                    pix = static_cast<int>(q);
+                    pix = static_cast<int>(kList ? list[q] : q);  // kList: the listed sample
                     smp = 0;
                     acc[0] = acc[1] = acc[2] = 0.0;
                 } else {
@@ -86,11 +94,13 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             }
         }
         if (!live && pix >= 0) {
-            const int qx = pix % tile.w, qy = pix / tile.w;
+            const int pixel = kList ? pix / grid2 : pix;
+            const int s = kList ? pix % grid2 : smp;
+            const int qx = pixel % tile.w, qy = pixel / tile.w;
             const int i = tile.x0 + qx, j = tile.y0 + qy * tile.row_step;
-            const int sy = smp / S.grid, sx = smp % S.grid;
-            const double x = i + (sx + pixel_hash(i, j, smp, 0)) * S.cell;
-            const double yy = j + (sy + pixel_hash(i, j, smp, 1)) * S.cell;
+            const int sy = s / S.grid, sx = s % S.grid;
+            const double x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
+            const double yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;
             double p[4];
             camera_momentum(S, x, yy, p);
             y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], p[1], p[2]};
@@ -230,10 +240,12 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
         // ---- finish a terminated sample ----
         if (live && term >= 0) {
             live = false;
-            ++cnt.rays;
-            if (term == kTermEscaped) ++cnt.escaped;
-            else if (term == kTermHorizon) ++cnt.horizon;
-            else ++cnt.maxsteps;
+            if (!kList) {
+                ++cnt.rays;
+                if (term == kTermEscaped) ++cnt.escaped;
+                else if (term == kTermHorizon) ++cnt.horizon;
+                else ++cnt.maxsteps;
+            }
             double col[3];
             for (int ch = 0; ch < 3; ++ch) {
                 const double nu = rgb_nu(ch);
@@ -243,24 +255,32 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
                 const double bright = star_brightness(S.stars, y.th, y.ph);
                 for (int ch = 0; ch < 3; ++ch) col[ch] += bright;
             }
-            for (int ch = 0; ch < 3; ++ch) acc[ch] = acc[ch] + col[ch];
-            if (out_fate) {
+            if (kList) {
+                const size_t q = static_cast<size_t>(pix);
+                for (int ch = 0; ch < 3; ++ch) out_d[3 * q + ch] = col[ch];
                 const unsigned ne = (entries > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(entries);
-                out_fate[static_cast<size_t>(pix) * grid2 + smp] = static_cast<unsigned>(term) | (ne << 2);
-            }
-            if (++smp == grid2) {
-                const int qx = pix % tile.w, qy = pix / tile.w;
-                const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
-                const double r0 = acc[0] * S.inv_spp, r1 = acc[1] * S.inv_spp, r2 = acc[2] * S.inv_spp;
-                if (out_rgba)
-                    out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1), static_cast<float>(r2),
-                                              1.0f);
-                if (out_d) {
-                    out_d[3 * o + 0] = r0;
-                    out_d[3 * o + 1] = r1;
-                    out_d[3 * o + 2] = r2;
-                }
+                out_fate[q] = static_cast<unsigned>(term) | (ne << 2);
                 pix = -1;
+            } else {
+                for (int ch = 0; ch < 3; ++ch) acc[ch] = acc[ch] + col[ch];
+                if (out_fate) {
+                    const unsigned ne = (entries > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(entries);
+                    out_fate[static_cast<size_t>(pix) * grid2 + smp] = static_cast<unsigned>(term) | (ne << 2);
+                }
+                if (++smp == grid2) {
+                    const int qx = pix % tile.w, qy = pix / tile.w;
+                    const size_t o = static_cast<size_t>(qy) * tile.out_pitch + qx;
+                    const double r0 = acc[0] * S.inv_spp, r1 = acc[1] * S.inv_spp, r2 = acc[2] * S.inv_spp;
+                    if (out_rgba)
+                        out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1),
+                                                  static_cast<float>(r2), 1.0f);
+                    if (out_d) {
+                        out_d[3 * o + 0] = r0;
+                        out_d[3 * o + 1] = r1;
+                        out_d[3 * o + 2] = r2;
+                    }
+                    pix = -1;
+                }
             }
         }
 
@@ -278,26 +298,46 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
     flush_vol(stats, cnt, cancelled);
 }
 
-cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                              const LaunchResources& res, int form, cudaStream_t stream) {
-    (void)form;  // the FP64 method serves both forms (see the file comment)
-    static int blocks_per_sm = 0, num_sms = 0;
-    if (blocks_per_sm == 0) {
+namespace {
+int vol_rgb_blocks_per_sm(bool list, int& sms) {
+    static int per[2] = {0, 0}, num_sms = 0;
+    if (num_sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, vol_render_kernel, kVolThreads, 0);
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], vol_render_kernel<false>, kVolThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], vol_render_kernel<true>, kVolThreads, 0);
+        for (int& p : per)
+            if (p < 1) p = 1;
     }
+    sms = num_sms;
+    return per[list ? 1 : 0];
+}
+}  // namespace
+
+cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                              const LaunchResources& res, cudaStream_t stream) {
+    int sms = 0;
+    const int per = vol_rgb_blocks_per_sm(false, sms);
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
     if (total == 0) return cudaSuccess;
-    int blocks = num_sms * blocks_per_sm;
+    int blocks = sms * per;
     const int needed = static_cast<int>((total + kVolThreads - 1) / kVolThreads);
     if (needed < blocks) blocks = needed;
     cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    vol_render_kernel<<<blocks, kVolThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
-                                                          res.stats, res.cancel);
+    vol_render_kernel<false><<<blocks, kVolThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
+                                                                 res.stats, res.cancel, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_volume_rgb_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
+                                      DevStats* stats, const volatile int* cancel, cudaStream_t stream) {
+    int sms = 0;
+    const int per = vol_rgb_blocks_per_sm(true, sms);
+    vol_render_kernel<true><<<sms * per, kVolThreads, 0, stream>>>(S, tile, nullptr, mb.sample_rgb, mb.sample_fate,
+                                                                   mb.queue2, stats, cancel, mb.retrace_list,
+                                                                   mb.retrace_count);
     return cudaGetLastError();
 }
 

@@ -436,11 +436,20 @@ __device__ __forceinline__ bool vol_reach(const VolReach& v, const ReachRay& rr,
     return fmax(r_lo - pad, 0.0) * c_lo - pad <= v.Z;
 }
 
+// kRGB = false (spectral): a settled sample gets its fate in out_fate (the
+// spectra, zeroed, carry no sky). kRGB = true: the mixed form's sample
+// buffers of the RGB render: a settled sample gets colour 0 and its fate, or,
+// escaping under a star sky, its sky arc for the star pass (mixed_star_kernel)
+// in sample_rgb and kFateStarPending; rays are counted here and terminations
+// by the resolve, as in the thin-disk mixed form.
+template <bool kRGB>
 __global__ void __launch_bounds__(kSpecThreads, 4)
 vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, const VolReach reach,
                      uint32_t* __restrict__ out_fate, unsigned* __restrict__ queue,
-                     unsigned* __restrict__ list, unsigned* __restrict__ list_count, DevStats* __restrict__ stats) {
+                     unsigned* __restrict__ list, unsigned* __restrict__ list_count, double* __restrict__ sample_rgb,
+                     DevStats* __restrict__ stats) {
     const int lane = threadIdx.x & 31;
+    const bool sky = kRGB && S.stars_on;  // escapes look a star up: no early ends
     const int g2 = S.grid * S.grid;
     const unsigned total = static_cast<unsigned>(tile.w) * tile.h * g2;
     const float Mf = static_cast<float>(S.M), af = static_cast<float>(S.a);
@@ -497,7 +506,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
             else if (y.r > S.r_escape) term = kTermEscaped;
             // never inside R: a turning point there, so it escapes, and the
             // plain stepping it gets has zero intensity; nothing to trace
-            else if (step == 0 && rr.far) term = kTermEscaped;
+            else if (!sky && step == 0 && rr.far) term = kTermEscaped;
         }
         if (live && term < 0) {
             if (!k1_ok) {
@@ -520,11 +529,11 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
                 ++step;
                 if (retrace)
                     term = kTermMaxSteps;
-                else if (mixed::certain_escape(y,
+                else if (!sky && mixed::certain_escape(y,
                                                fmax(fmax(mixed::kEscapeRMin * S.M, S.r_near_mixed),
                                                     reach.R + 2.0 * reach.margin + 2e-3 * y.r),
                                                step, S.max_steps))
-                    term = kTermEscaped;  // spectra carry no sky: the escape is final once certain
+                    term = kTermEscaped;  // no sky lookup: the escape is final once certain
             } else {
                 dl = d.next;
                 ++retry;
@@ -533,8 +542,24 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
         bool queue_it = false;
         if (live && term >= 0) {
             live = false;
+            if (kRGB) ++cnt.rays;
             if (retrace || term == kTermMaxSteps) {
                 queue_it = true;
+            } else if (kRGB) {
+                const size_t o = 3 * static_cast<size_t>(q);
+                if (term == kTermEscaped && S.stars_on) {
+                    // k1 is the FP32 right-hand side at the escape state
+                    const mixed::EscapeArc e = mixed::escape_arc(S.r_escape, y, k1);
+                    sample_rgb[o + 0] = e.th0;
+                    sample_rgb[o + 1] = e.ph0;
+                    sample_rgb[o + 2] = __hiloint2double(__float_as_int(e.dth), __float_as_int(e.dph));
+                    out_fate[q] = mixed::kFateStarPending;
+                } else {
+                    sample_rgb[o + 0] = 0.0;
+                    sample_rgb[o + 1] = 0.0;
+                    sample_rgb[o + 2] = 0.0;
+                    out_fate[q] = static_cast<unsigned>(term);
+                }
             } else {
                 ++cnt.rays;
                 if (term == kTermEscaped) ++cnt.escaped;
@@ -577,7 +602,7 @@ __global__ void vol_resolve_kernel(const __grid_constant__ DevScene S, const Dev
 // ---------------------------------------------------------------------------
 namespace {
 struct SpecShape {
-    int sms = 0, per_fp64 = 1, per_list = 1, per_spec = 1;
+    int sms = 0, per_fp64 = 1, per_list = 1, per_spec = 1, per_spec_rgb = 1;
 };
 const SpecShape& spec_shape() {
     static SpecShape sh;
@@ -587,7 +612,9 @@ const SpecShape& spec_shape() {
         cudaDeviceGetAttribute(&sh.sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_fp64, vol_spectral_kernel<false>, kSpecThreads, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_list, vol_spectral_kernel<true>, kSpecThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, vol_speculate_kernel, kSpecThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, vol_speculate_kernel<false>, kSpecThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec_rgb, vol_speculate_kernel<true>, kSpecThreads, 0);
+        if (sh.per_spec_rgb < 1) sh.per_spec_rgb = 1;
         if (sh.per_fp64 < 1) sh.per_fp64 = 1;
         if (sh.per_list < 1) sh.per_list = 1;
         if (sh.per_spec < 1) sh.per_spec = 1;
@@ -666,8 +693,8 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     const int need = static_cast<int>((n + kSpecThreads - 1) / kSpecThreads);
     int sb = sh.sms * sh.per_spec;
     if (need < sb) sb = need;
-    vol_speculate_kernel<<<sb, kSpecThreads, 0, stream>>>(S, tile, reach, out.fate, res.queue, list, list_count,
-                                                         res.stats);
+    vol_speculate_kernel<false><<<sb, kSpecThreads, 0, stream>>>(S, tile, reach, out.fate, res.queue, list,
+                                                                list_count, nullptr, res.stats);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     mark(1);
@@ -684,6 +711,46 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     vol_resolve_kernel<<<rb, 256, 0, stream>>>(S, tile, freqs, nb, sample_spec, out.spec);
     e = cudaGetLastError();
     mark(3);
+    return e;
+}
+
+cudaError_t launch_volume_rgb_mixed(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                                    const LaunchResources& res, void* scratch, size_t scratch_bytes, double reach_z,
+                                    cudaEvent_t* phase_events, cudaStream_t stream) {
+    auto mark = [&](int k) {
+        if (phase_events) cudaEventRecord(phase_events[k], stream);
+    };
+    const SpecShape& sh = spec_shape();
+    const int g2 = S.grid * S.grid;
+    const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
+    if (n == 0) return cudaSuccess;
+    if (scratch_bytes < mixed_scratch_bytes(tile, g2)) return cudaErrorInvalidValue;
+    const DevMixedBuffers mb = mixed_buffers(scratch, n, res.queue);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 1024, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    VolReach reach;
+    reach.R = 1.5 * S.vol.r_outer;
+    reach.Z = reach_z;
+    reach.margin = S.mixed_margin;
+    mark(0);
+    const int need = static_cast<int>((n + kSpecThreads - 1) / kSpecThreads);
+    int sb = sh.sms * sh.per_spec_rgb;
+    if (need < sb) sb = need;
+    vol_speculate_kernel<true><<<sb, kSpecThreads, 0, stream>>>(S, tile, reach, mb.sample_fate, res.queue,
+                                                               mb.retrace_list, mb.retrace_count, mb.sample_rgb,
+                                                               res.stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    mark(1);
+    e = launch_mixed_stars(S, tile, mb, stream);
+    if (e != cudaSuccess) return e;
+    mark(2);
+    e = launch_volume_rgb_retrace(S, tile, mb, res.stats, res.cancel, stream);
+    if (e != cudaSuccess) return e;
+    mark(3);
+    e = launch_mixed_resolve(S, tile, mb, out, res.stats, stream);
+    mark(4);
     return e;
 }
 

@@ -54,11 +54,24 @@ def test_volumetric_mixed_equals_fp64(grrt, need_gpu, name, kw):
     assert share < 0.95
 
 
-def test_volumetric_rgb_mixed_is_fp64(grrt, need_gpu):
-    """The volumetric RGB render runs the FP64 method for both forms."""
-    R = grrt.Renderer(grrt.config_params(3, width=48, height=48))
+@pytest.mark.parametrize("bg", [0, 1], ids=["black sky", "stars"])
+def test_volumetric_rgb_mixed_equals_fp64(grrt, need_gpu, bg):
+    """The volumetric RGB render's mixed form (the same speculation, plus the
+    thin-disk form's star pass for escapes under a star sky, then the FP64
+    re-trace and the ordered resolve) gives the FP64 form's image and fates
+    bit for bit."""
+    from parity_util import device_render_rgb
+    R = grrt.Renderer(grrt.config_params(3, width=64, height=48, background_type=bg, samples_per_pixel=4))
     R.set_precision(grrt.FORM_FP64)
-    a = R.render()
+    f_rgba, f64, ffate, fst = device_render_rgb(R, 4)
     R.set_precision(grrt.FORM_MIXED)
-    b = R.render()
-    np.testing.assert_array_equal(a, b)
+    m_rgba, m64, mfate, mst = device_render_rgb(R, 4)
+    assert (f64 > 0).any()
+    np.testing.assert_array_equal(m64, f64)
+    np.testing.assert_array_equal(m_rgba, f_rgba)
+    np.testing.assert_array_equal(mfate, ffate)
+    assert mst["rays"] == fst["rays"] == 64 * 48 * 4
+    assert mst["horizon"] == fst["horizon"] and mst["escaped"] == fst["escaped"]
+    share = mst["fp64_attempts"] / fst["fp64_attempts"]
+    print(f"\n  [{'stars' if bg else 'black'}] re-traced FP64 attempts / FP64 form's {share:.3f}")
+    assert share < 0.95
