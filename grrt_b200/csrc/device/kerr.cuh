@@ -98,6 +98,20 @@ GRRT_HD void fast_sincos(float x, float& s, float& c) {
     c = flip_c ? -cv : cv;
 }
 
+// sin and cos for the right-hand side: the reference's polynomial in FP64; in
+// FP32 on the device the hardware approximations (__sincosf, two
+// special-function ops instead of the ~25 instructions of the polynomial; the
+// FP32 form's error budget absorbs their few-ulp error), the FP32 polynomial
+// on the host.
+GRRT_HD void rhs_sincos(double x, double& s, double& c) { fast_sincos(x, s, c); }
+GRRT_HD void rhs_sincos(float x, float& s, float& c) {
+#ifdef __CUDA_ARCH__
+    __sincosf(x, &s, &c);
+#else
+    fast_sincos(x, s, c);
+#endif
+}
+
 // 1/x: IEEE division in FP64; in FP32 the hardware reciprocal approximation
 // (about 1 ulp), which the FP32 form's error budget absorbs.
 GRRT_HD double recip(double x) { return 1.0 / x; }
@@ -116,7 +130,7 @@ GRRT_RHS_ATTR Vec5<T> kerr_rhs(T M, T a, T pt, T pph, const Vec5<T>& y) {
     using std::fabs;
     const T r = y.r, pr = y.pr, pth = y.pth;
     T s, c;
-    fast_sincos(y.th, s, c);
+    rhs_sincos(y.th, s, c);
     if (fabs(s) < T(1e-10)) s = (s >= T(0)) ? T(1e-10) : T(-1e-10);
     const T r2 = r * r, a2 = a * a;
     const T Sigma = r2 + a2 * c * c;
