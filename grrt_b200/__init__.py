@@ -118,6 +118,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_set_mixed_params": (C.c_int, [vp, C.c_double, C.c_double]),
         "grrt_render_device": (C.c_int, [vp, vp, vp, vp, vp]),
         "grrt_render_rows_device": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]),
+        "grrt_tonemap_device": (C.c_int, [vp, C.c_int, C.c_int, vp]),
         "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
@@ -589,6 +590,14 @@ def sweep_cameras(width: int = 256, height: int = 256, spins=(0.0, 0.5, 0.9, 0.9
                 p.update(spin=spin)
             cams.append(p)
     return cams
+
+
+def tonemap_device(d_rgba, width: int, height: int, stream=None) -> None:
+    """In-place tone mapping of a device RGBA float frame (raw pointer or torch tensor)."""
+    p = d_rgba if isinstance(d_rgba, int) else d_rgba.data_ptr()
+    s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+    if lib().grrt_tonemap_device(p, width, height, s) != 0:
+        raise RuntimeError("grrt_tonemap_device failed")
 
 
 def cuda_available() -> bool:

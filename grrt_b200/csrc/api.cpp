@@ -257,6 +257,17 @@ extern "C" GRRT_EXPORT void grrt_tonemap(float* fb, int width, int height) {
     }
 }
 
+// The same on the device, in place on a device frame, enqueued on `stream`.
+extern "C" GRRT_EXPORT int grrt_tonemap_device(float* d_rgba, int width, int height, void* stream) {
+    if (!d_rgba || width <= 0 || height <= 0) return -1;
+    const cudaError_t e = launch_tonemap(d_rgba, width, height, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return 0;
+}
+
 extern "C" GRRT_EXPORT void grrt_debug_pixel(GRRTContext* ctx, int px, int py) {
     if (!ctx) {
         std::printf("grrt_debug_pixel: context not ready\n");

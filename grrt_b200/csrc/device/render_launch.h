@@ -117,6 +117,9 @@ cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const D
 cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
                                  const ThinOutputs& out, DevStats* stats, cudaStream_t stream);
 
+// In-place tone mapping of a device RGBA float frame (tonemap.cu; 16-byte aligned).
+cudaError_t launch_tonemap(float* d_rgba, int width, int height, cudaStream_t stream);
+
 // Batched thin-disk render over many cameras (see DevBatch), FP64 form.
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats,
                               int blocks, cudaStream_t stream);

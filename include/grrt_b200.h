@@ -81,6 +81,12 @@ GRRT_EXPORT int grrt_render_device(GRRTContext* ctx, float* d_rgba, double* d_rg
 GRRT_EXPORT int grrt_render_rows_device(GRRTContext* ctx, int row0, int row_step, int n_rows, float* d_rgba,
                                         double* d_rgb64, unsigned int* d_fate, void* stream);
 
+/* Tone mapping of a device RGBA float frame in place (the reference's
+ * grrt_tonemap: log-average auto exposure, extended Reinhard, gamma 2.2),
+ * enqueued on `stream`. d_rgba 16-byte aligned. Agrees with grrt_tonemap on
+ * the host to a few float ulp (the log sum is grouped by blocks). 0 or -1. */
+GRRT_EXPORT int grrt_tonemap_device(float* d_rgba, int width, int height, void* stream);
+
 /* Spectral render into device memory (Renderer::render_spectral,
  * src/renderer.cpp:84-138): d_spec double[width*height*bins]. */
 GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double* d_spec, int width, int height,
