@@ -37,6 +37,17 @@ BG_STARS = 1
 BG_TEXTURE = 2
 
 
+DEBUG_START, DEBUG_STEP, DEBUG_THIN_HIT, DEBUG_MARCH_ENTRY, DEBUG_MARCH_EXIT, DEBUG_END = range(6)
+DEBUG_EVENT_NONE, DEBUG_EVENT_CROSS, DEBUG_EVENT_INSIDE, DEBUG_EVENT_NEAR = range(4)
+
+
+class GRRTDebugRecord(C.Structure):
+    """Mirror of GRRTDebugRecord (include/grrt_b200.h)."""
+
+    _fields_ = [("kind", C.c_int), ("step", C.c_int), ("event", C.c_int), ("aux", C.c_int),
+                ("v", C.c_double * 7)]
+
+
 class GRRTParams(C.Structure):
     """Mirror of GRRTParams (include/grrt/types.h:20-64, include/grrt_api.h)."""
 
@@ -158,6 +169,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_batch_get_stats": (C.c_int, [vp, P(GRRTStats)]),
         "grrt_scene_table": (C.c_longlong, [vp, C.c_char_p, P(C.c_double), C.c_longlong]),
         "grrt_camera_ray": (C.c_int, [vp, C.c_double, C.c_double, P(C.c_double)]),
+        "grrt_debug_trace": (C.c_int, [vp, C.c_double, C.c_double, P(GRRTDebugRecord), C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -369,6 +381,27 @@ class Renderer:
         out = np.empty(8, dtype=np.float64)
         self._L.grrt_camera_ray(self.ctx, x, y, _dptr(out))
         return out
+
+    def debug_trace(self, x: float, y: float, capacity: Optional[int] = None) -> list:
+        """The FP64 device trace of the sample at fractional pixel (x, y) as
+        records (grrt_debug_trace): dicts with kind, step, event, aux and v."""
+        if capacity is None:
+            n = self._L.grrt_debug_trace(self.ctx, x, y, None, 0)
+            if n < 0:
+                err = self._L.grrt_error(self.ctx)
+                raise RuntimeError("grrt_debug_trace failed: " + (err.decode() if err else f"rc={n}"))
+            capacity = n
+        buf = (GRRTDebugRecord * max(1, capacity))()
+        n = self._L.grrt_debug_trace(self.ctx, x, y, buf, capacity)
+        if n < 0:
+            err = self._L.grrt_error(self.ctx)
+            raise RuntimeError("grrt_debug_trace failed: " + (err.decode() if err else f"rc={n}"))
+        return [{"kind": r.kind, "step": r.step, "event": r.event, "aux": r.aux, "v": list(r.v)}
+                for r in buf[:min(n, capacity)]]
+
+    def debug_pixel(self, px: int, py: int) -> None:
+        """Print the pixel centre's trace (grrt_debug_pixel) to the process's stdout."""
+        self._L.grrt_debug_pixel(self.ctx, px, py)
 
 
 class Batch:

@@ -347,3 +347,9 @@ extern "C" GRRT_EXPORT int grrt_camera_ray(const GRRTContext* ctx, double x, dou
     camera_ray(ctx->cam, x, y, out, out + 4);
     return 0;
 }
+
+extern "C" GRRT_EXPORT int grrt_debug_trace(GRRTContext* ctx, double x, double y, GRRTDebugRecord* records,
+                                            int capacity) {
+    if (!ctx || capacity < 0 || (capacity > 0 && !records)) return -1;
+    return ctx->debug_trace(x, y, records, capacity);
+}

@@ -658,47 +658,89 @@ bool GRRTContext::export_table(const std::string& name, std::vector<double>& v) 
     return false;
 }
 
+int GRRTContext::debug_trace(double x, double y, GRRTDebugRecord* out, int capacity) {
+    static_assert(sizeof(GRRTDebugRecord) == sizeof(DevDebugRecord), "debug record layout");
+    static_assert(GRRT_DEBUG_START == kDebugStart && GRRT_DEBUG_STEP == kDebugStep &&
+                      GRRT_DEBUG_THIN_HIT == kDebugThinHit && GRRT_DEBUG_MARCH_ENTRY == kDebugMarchEntry &&
+                      GRRT_DEBUG_MARCH_EXIT == kDebugMarchExit && GRRT_DEBUG_END == kDebugEnd &&
+                      GRRT_DEBUG_EVENT_CROSS == kDebugCross && GRRT_DEBUG_EVENT_INSIDE == kDebugInside &&
+                      GRRT_DEBUG_EVENT_NEAR == kDebugNear,
+                  "debug record codes");
+    if (!ensure_device()) return -1;
+    const int want = (out && capacity > 0) ? capacity : 1;
+    const int cap = std::max(1, std::min(debug_trace_capacity(max_steps), want));
+    void* d_buf = nullptr;
+    const size_t rec_bytes = sizeof(DevDebugRecord) * static_cast<size_t>(cap);
+    if (fail_cuda(cudaMalloc(&d_buf, rec_bytes + sizeof(int)), "cudaMalloc(debug trace)")) return -1;
+    auto* d_rec = static_cast<DevDebugRecord*>(d_buf);
+    int* d_count = reinterpret_cast<int*>(static_cast<char*>(d_buf) + rec_bytes);
+    int n = -1;
+    cudaError_t e = launch_debug_trace(scene_for_launch(), x, y, d_rec, cap, d_count, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&n, d_count, sizeof n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && out && capacity > 0 && n > 0)
+        e = cudaMemcpy(out, d_rec, sizeof(DevDebugRecord) * static_cast<size_t>(std::min(n, cap)),
+                       cudaMemcpyDeviceToHost);
+    cudaFree(d_buf);
+    if (fail_cuda(e, "debug trace")) return -1;
+    return n;
+}
+
 void GRRTContext::debug_pixel(int px, int py) {
-    // Trace the pixel centre on the device and report its fate and colour.
-    double init[8];
-    camera_ray(cam, px + 0.5, py + 0.5, init, init + 4);
-    std::printf("=== DEBUG PIXEL TRACE ===\n  r0=%.4f theta0=%.6f phi0=%.4f\n", init[1], init[2], init[3]);
-    std::printf("  p0=(%+.4e %+.4e %+.4e %+.4e)\n", init[4], init[5], init[6], init[7]);
-    if (!ensure_device()) {
-        std::printf("  (no device: %s)\n", error.c_str());
+    // The pixel centre's FP64 trace on the device, printed in the layout of
+    // GeodesicTracer::trace_debug (src/geodesic_tracer.cpp:339-493).
+    const int cap = debug_trace_capacity(max_steps);
+    std::vector<GRRTDebugRecord> rec(static_cast<size_t>(cap));
+    const int n = debug_trace(px + 0.5, py + 0.5, rec.data(), cap);
+    std::printf("=== DEBUG PIXEL TRACE ===\n");
+    if (n < 1) {
+        std::printf("  (device trace failed: %s)\n", error.c_str());
+        std::fflush(stdout);
         return;
     }
-    int grid = std::max(1, static_cast<int>(std::sqrt(static_cast<double>(spp))));
-    DevTile tile;
-    tile.x0 = px;
-    tile.y0 = py;
-    tile.w = 1;
-    tile.h = 1;
-    tile.out_pitch = 1;
-    double* d_rgb = nullptr;
-    unsigned* d_fate = nullptr;
-    if (cudaMalloc(&d_rgb, sizeof(double) * 3) != cudaSuccess ||
-        cudaMalloc(&d_fate, sizeof(unsigned) * grid * grid) != cudaSuccess) {
-        cudaGetLastError();
-        cudaFree(d_rgb);
-        std::printf("  (allocation failed)\n");
-        return;
+    const int shown = std::min(n, cap);
+    const GRRTDebugRecord& s0 = rec[0];
+    std::printf("  r0=%.4f theta0=%.6f phi0=%.4f\n", s0.v[0], s0.v[1], s0.v[2]);
+    std::printf("  p0=(%+.4e %+.4e %+.4e %+.4e)\n", s0.v[3], s0.v[4], s0.v[5], s0.v[6]);
+    if (vol) std::printf("  disk: r_in=%.3f r_out=%.3f r_isco=%.3f\n", vol->r_horizon, vol->r_outer, vol->r_isco);
+    std::printf("%-6s %-10s %-10s %-10s %-12s %-8s %-8s %-6s\n", "step", "r", "theta", "z", "dlambda", "H", "zm",
+                "event");
+    std::printf("%s %s %s %s %s %s %s %s\n", "------", "----------", "----------", "----------", "------------",
+                "--------", "--------", "------");
+    static const char* events[] = {"  ", "CROSS", "INSIDE", "NEAR"};
+    for (int k = 1; k < shown; ++k) {
+        const GRRTDebugRecord& r = rec[k];
+        switch (r.kind) {
+            case GRRT_DEBUG_STEP:
+                if (vol)
+                    std::printf("%-6d %-10.4f %-10.6f %-10.4f %-12.4e %-8.4f %-8.4f %s\n", r.step, r.v[0], r.v[1],
+                                r.v[2], r.v[3], r.v[4], r.v[5], events[r.event & 3]);
+                else
+                    std::printf("%-6d %-10.4f %-10.6f %-10.4f %-12.4e %-8s %-8s %s\n", r.step, r.v[0], r.v[1],
+                                r.v[2], r.v[3], "-", "-", events[0]);
+                break;
+            case GRRT_DEBUG_THIN_HIT:
+                std::printf("  -> THIN DISK HIT r_cross=%.4f emit=(%.4e %.4e %.4e)\n", r.v[0], r.v[1], r.v[2], r.v[3]);
+                break;
+            case GRRT_DEBUG_MARCH_ENTRY:
+                std::printf("  -> RAYMARCH entry r=%.4f z=%.4f\n", r.v[0], r.v[1]);
+                break;
+            case GRRT_DEBUG_MARCH_EXIT:
+                std::printf("  -> RAYMARCH exit  color=(%.4e %.4e %.4e)\n", r.v[0], r.v[1], r.v[2]);
+                break;
+            case GRRT_DEBUG_END:
+                if (shown < n) std::printf("  ... %d record(s) not shown\n", n - shown);
+                if (r.event == 0)
+                    std::printf("%-6d %-10.4f  -> HORIZON\n", r.step, r.v[0]);
+                else if (r.event == 1)
+                    std::printf("%-6d %-10.4f  -> ESCAPED\n", r.step, r.v[0]);
+                else
+                    std::printf("  -> MAX STEPS  color=(%.4e %.4e %.4e)\n", r.v[3], r.v[4], r.v[5]);
+                std::printf("  color=(%.4e %.4e %.4e) after %.0f attempts\n", r.v[3], r.v[4], r.v[5], r.v[6]);
+                break;
+            default:
+                break;
+        }
     }
-    if (render_rgb_device(tile, nullptr, d_rgb, d_fate, stream, true) == 0 && cudaStreamSynchronize(stream) == cudaSuccess) {
-        double rgb[3];
-        std::vector<unsigned> fate(grid * grid);
-        cudaMemcpy(rgb, d_rgb, sizeof rgb, cudaMemcpyDeviceToHost);
-        cudaMemcpy(fate.data(), d_fate, sizeof(unsigned) * fate.size(), cudaMemcpyDeviceToHost);
-        GRRTStats st{};
-        read_stats(&st);
-        static const char* names[] = {"HORIZON", "ESCAPED", "MAX STEPS"};
-        for (size_t s = 0; s < fate.size(); ++s)
-            std::printf("  sample %zu -> %s after crossing the disk %u time(s)\n", s, names[fate[s] & 3u], fate[s] >> 2);
-        std::printf("  accepted steps %llu, attempts %llu\n", st.accepted, st.attempts);
-        std::printf("  color=(%.4e %.4e %.4e)\n", rgb[0], rgb[1], rgb[2]);
-    } else {
-        std::printf("  render failed: %s\n", error.c_str());
-    }
-    cudaFree(d_rgb);
-    cudaFree(d_fate);
+    std::fflush(stdout);
 }

@@ -88,6 +88,7 @@ struct GRRTContext {
     int read_stats(GRRTStats* out);
     int phase_ms(double* out, int cap);
     bool export_table(const std::string& name, std::vector<double>& out) const;
+    int debug_trace(double x, double y, GRRTDebugRecord* out, int capacity);
     void debug_pixel(int px, int py);
     void request_cancel();
 

@@ -120,6 +120,24 @@ cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const D
 // In-place tone mapping of a device RGBA float frame (tonemap.cu; 16-byte aligned).
 cudaError_t launch_tonemap(float* d_rgba, int width, int height, cudaStream_t stream);
 
+// One record of the single-ray debug trace (debug_trace.cu); the layout and
+// the codes are GRRTDebugRecord's and its GRRT_DEBUG_* values.
+struct DevDebugRecord {
+    int kind, step, event, aux;
+    double v[7];
+};
+constexpr int kDebugStart = 0, kDebugStep = 1, kDebugThinHit = 2, kDebugMarchEntry = 3, kDebugMarchExit = 4,
+              kDebugEnd = 5;
+constexpr int kDebugNone = 0, kDebugCross = 1, kDebugInside = 2, kDebugNear = 3;
+constexpr int kDebugMaxRecords = 1 << 20;
+// Records a trace of at most max_steps outer steps can produce (bounded by kDebugMaxRecords).
+int debug_trace_capacity(int max_steps);
+// Trace the camera sample at fractional pixel (x, y) in FP64 into rec[0 .. cap)
+// (the last slot holds the END record when the trace has more); *count
+// receives the number of records the trace produced.
+cudaError_t launch_debug_trace(const DevScene& S, double x, double y, DevDebugRecord* rec, int cap, int* count,
+                               cudaStream_t stream);
+
 // Batched thin-disk render over many cameras (see DevBatch), FP64 form.
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats,
                               int blocks, cudaStream_t stream);

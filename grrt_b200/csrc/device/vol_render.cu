@@ -28,12 +28,6 @@ namespace {
 constexpr int kVolThreads = 128;
 constexpr unsigned kFullMask = 0xffffffffu;
 
-// Observer-frame RGB frequencies (450, 550, 650 nm) of the RGB transfer.
-__device__ __forceinline__ double rgb_nu(int ch) {
-    constexpr double c = 2.997924e10;
-    return ch == 0 ? c / 450e-7 : (ch == 1 ? c / 550e-7 : c / 650e-7);
-}
-
 }  // namespace
 
 // Three channels in registers; the march ends when all T < 1e-6.
@@ -167,67 +161,8 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
             }
         } else if (live && term < 0 && marching) {
             // ---- one RK4 march step ----
-            const Vec5<double> ns = rk4_step<double>(S.M, S.a, pt, pph, ms, ds);
+            bool end = vol_march_rgb_step(S, pt, pph, ms, ds, been_inside, J, Tt, cnt);
             ++mcount;
-            ++cnt.march;
-            const double r = ns.r, theta = ns.th;
-            double st, ct;
-            sincos(theta, &st, &ct);
-            const double z = r * ct;
-            bool end = false;
-            if (r < V.r_horizon || r > V.r_outer) {
-                end = true;
-            } else if (Tt[0] < 1e-6 && Tt[1] < 1e-6 && Tt[2] < 1e-6) {
-                end = true;
-            } else {
-                const double H = v_scale_height(V, r);
-                if (!v_inside(V, r, z)) {
-                    const double zm = v_zmax(V, r);
-                    if (been_inside && fabs(z) > zm + 3.0 * H) {
-                        end = true;
-                    } else if (!been_inside) {
-                        ds = vmax(vmin(fabs(z) / 8.0, H * 2.0), H / 64.0);
-                    } else {
-                        ds = vclamp(H / 4.0, H / 64.0, H);
-                    }
-                } else {
-                    been_inside = true;
-                    const double rho = v_density(V, V.perm, r, z, ns.ph);
-                    const double Tl = v_temperature(V, r, fabs(z));
-                    if (rho > 0.0 && Tl > 0.0) {
-                        ++cnt.physics;
-                        double g, pue;
-                        v_redshift(V, pt, ns.pr, pph, r, theta, g, pue);
-                        const double dsp = fabs(pue) * fabs(ds);
-                        int ir, iT;
-                        double fr, fT;
-                        log_locate(log10(rho), V.log_rho_min, V.log_rho_max, V.n_rho, ir, fr);
-                        log_locate(log10(Tl), V.log_T_min, V.log_T_max, V.n_T, iT, fT);
-                        const double ke = v_kappa_es(V, ir, fr, iT, fT);
-                        const double ag = fabs(g);
-                        double ka_med = 0.0;
-                        for (int b = 0; b < 3; ++b) {
-                            const double nu = ag * rgb_nu(b);
-                            const double ka = v_kappa_abs(V, nu, ir, fr, iT, fT);
-                            if (b == 1) ka_med = ka;
-                            const double kt = ka + ke;
-                            const double eps = (kt > 0.0) ? ka / kt : 1.0;
-                            const double dtau = kt * rho * dsp;
-                            const double B = planck_nu(nu, Tl);
-                            const double Sv = eps * B / (nu * nu * nu);
-                            const double e = exp(-dtau);
-                            J[b] += Tt[b] * Sv * (1.0 - e);
-                            Tt[b] *= e;
-                        }
-                        cnt.bins += 3;
-                        const double at = (ka_med + ke) * rho;
-                        const double ds_tau = (at > 0.0) ? 0.05 / at : ds * 2.0;
-                        const double ds_geo = 0.1 * vmax(r - V.r_horizon, 0.5);
-                        ds = vclamp(vmin(ds_tau, ds_geo), H / 64.0, H);
-                    }
-                }
-            }
-            ms = ns;
             if (!end && mcount >= 4096) end = true;
             if (end) {
                 marching = false;

@@ -26,7 +26,9 @@ extern "C" {
  * whose colour depends on the FP64 step sequence (emitting crossings, grazes,
  * near-critical orbits, escapes with a star in reach, the step budget) are
  * re-traced with the FP64 method, all others are exactly 0. MIXED, volumetric
- * disk: FP32 right-hand sides while the ray is far from the hole. */
+ * disk: samples whose FP32 trajectory provably stays away from the volume are
+ * finished by that pass (escape or horizon, no emission); every other sample
+ * is re-traced in FP64, so the output equals the FP64 form's bit for bit. */
 #define GRRT_FORM_FP64 0
 #define GRRT_FORM_MIXED 1
 
@@ -170,6 +172,46 @@ GRRT_EXPORT long long grrt_scene_table(const GRRTContext* ctx, const char* name,
  * Camera::ray_for_pixel (src/camera.cpp:69-96) evaluated on the host.
  * out[8] = (t, r, theta, phi, p_t, p_r, p_theta, p_phi). */
 GRRT_EXPORT int grrt_camera_ray(const GRRTContext* ctx, double x, double y, double* out);
+
+/* Single-ray debug trace: the FP64 trace of the camera sample at fractional
+ * pixel (x, y), run on the device, as the records of the lines
+ * GeodesicTracer::trace_debug prints (src/geodesic_tracer.cpp:339-493);
+ * grrt_debug_pixel prints them in that layout for the pixel centre.
+ *   START      v: r, theta, phi, p_t, p_r, p_theta, p_phi (the device's initial state)
+ *   STEP       one accepted outer step (step = its loop index); v: r, theta,
+ *              z, next dlambda, H, z_max, phi (H and z_max NaN without a
+ *              volumetric disk); event: GRRT_DEBUG_EVENT_* (volumetric)
+ *   THIN_HIT   an emitting thin-disk crossing; v: r_cross, emission r, g, b
+ *   MARCH_ENTRY a ray-march starts; v: r, z of its first state
+ *   MARCH_EXIT the ray-march ended; aux: its RK4 steps; v: the volume's colour
+ *              so far (J nu^3 per channel), r, z of its last state
+ *   END        event: termination (0 horizon, 1 escaped, 2 step budget);
+ *              aux: emitting crossings or ray-march entries; v: r, theta, phi,
+ *              colour r, g, b (disk and volume only: no sky), attempts. */
+#define GRRT_DEBUG_START 0
+#define GRRT_DEBUG_STEP 1
+#define GRRT_DEBUG_THIN_HIT 2
+#define GRRT_DEBUG_MARCH_ENTRY 3
+#define GRRT_DEBUG_MARCH_EXIT 4
+#define GRRT_DEBUG_END 5
+#define GRRT_DEBUG_EVENT_NONE 0
+#define GRRT_DEBUG_EVENT_CROSS 1
+#define GRRT_DEBUG_EVENT_INSIDE 2
+#define GRRT_DEBUG_EVENT_NEAR 3
+
+typedef struct {
+    int kind;   /* GRRT_DEBUG_* */
+    int step;
+    int event;
+    int aux;
+    double v[7];
+} GRRTDebugRecord;
+
+/* Run the debug trace; copies the first min(n, capacity) records into
+ * records (when n > capacity the last slot holds the END record) and returns
+ * n, the number of records of the trace, or -1 on an error (grrt_error).
+ * Synchronises the context's stream. */
+GRRT_EXPORT int grrt_debug_trace(GRRTContext* ctx, double x, double y, GRRTDebugRecord* records, int capacity);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,152 @@
+"""Single-ray debug trace (grrt_debug_trace, grrt_debug_pixel) against the oracle.
+
+The device trace of a pixel centre, recorded step by step, must describe the
+ray the oracle traces from the same sample: the same termination, the same
+number of accepted outer steps and attempts, the same emitting crossings or
+ray-march entries, and the same colour (the disk's and the volume's emission;
+the debug trace adds no sky, as GeodesicTracer::trace_debug,
+src/geodesic_tracer.cpp:339-493). Pixels are taken where the oracle's strict
+and FMA-contracted builds agree (outside the rounding-sensitive band), so a
+fate or colour difference is a bug, not rounding.
+grrt_debug_pixel prints the records in trace_debug's layout.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+COLOUR_TOL = 1e-6
+
+
+def stable_centres(R, candidates, want: int, spread: float):
+    """Pixel centres whose oracle traces agree between the strict and the FMA
+    build: same fate, colours within `spread` relative."""
+    import oracle_bind
+    xs = np.array([c[0] + 0.5 for c in candidates])
+    ys = np.array([c[1] + 0.5 for c in candidates])
+    O, F = oracle_bind.Oracle(R), oracle_bind.Oracle(R, fma=True)
+    rgb, term, nc, fin, _ = O.trace_rgb(xs, ys)
+    rgb2, term2, nc2, _, _ = F.trace_rgb(xs, ys)
+    ok = (term == term2) & (nc == nc2) & np.all(np.abs(rgb - rgb2) <= spread * np.abs(rgb) + 1e-300, axis=1)
+    # and the same accepted steps and attempts (a ray ending near the escape
+    # radius can take one step more in one build with the same colour)
+    for k in np.nonzero(ok)[0]:
+        c1 = O.trace_rgb(xs[k:k + 1], ys[k:k + 1])[4]
+        c2 = F.trace_rgb(xs[k:k + 1], ys[k:k + 1])[4]
+        ok[k] = c1["accepted"] == c2["accepted"] and c1["attempts"] == c2["attempts"]
+    # an even share of each fate class (termination, lit or not), spread over the image
+    groups = {}
+    for k in range(len(xs)):
+        if ok[k]:
+            groups.setdefault((int(term[k]), int(nc[k]) > 0), []).append(k)
+    per = max(1, want // max(1, len(groups)))
+    picked = []
+    for ks in groups.values():
+        picked += ks[:: max(1, len(ks) // per)][:per]
+    return O, [(xs[k], ys[k]) for k in sorted(picked)]
+
+
+def check_against_oracle(grrt, R, O, x, y):
+    rec = R.debug_trace(x, y)
+    kinds = [r["kind"] for r in rec]
+    assert kinds[0] == grrt.DEBUG_START and kinds[-1] == grrt.DEBUG_END
+    assert kinds.count(grrt.DEBUG_START) == 1 and kinds.count(grrt.DEBUG_END) == 1
+    # the device's initial state is the host camera's
+    init = R.camera_ray(x, y)
+    np.testing.assert_allclose(rec[0]["v"][:3], init[1:4], rtol=1e-14, atol=1e-15)
+    np.testing.assert_allclose(rec[0]["v"][3:], init[4:], rtol=1e-12, atol=1e-15)
+    rgb, term, nc, fin, cnt = O.trace_rgb(np.array([x]), np.array([y]))
+    end = rec[-1]
+    steps = [r for r in rec if r["kind"] == grrt.DEBUG_STEP]
+    assert [r["step"] for r in steps] == list(range(len(steps)))
+    assert end["step"] == len(steps)
+    assert end["event"] == term[0], (x, y)
+    assert end["aux"] == nc[0], (x, y)
+    assert len(steps) == cnt["accepted"], (x, y, len(steps), cnt)
+    assert int(end["v"][6]) == cnt["attempts"], (x, y, end["v"][6], cnt)
+    # final position: an escaping ray's last step spans hundreds of M, so its
+    # end radius carries last-bit differences of the step length (~1e-6)
+    np.testing.assert_allclose(end["v"][0], fin[0, 1], rtol=1e-4)
+    np.testing.assert_allclose(end["v"][1:3], fin[0, 2:4], rtol=1e-6, atol=1e-9)
+    colour = np.array(end["v"][3:6])
+    assert np.all(np.abs(colour - rgb[0]) <= COLOUR_TOL * np.abs(rgb[0]) + 1e-300), (colour, rgb[0])
+    return rec, term[0], nc[0]
+
+
+def test_debug_trace_thin_disk(grrt, need_gpu):
+    R = grrt.Renderer(grrt.config_params(2, width=64, height=64, background_type=0))
+    cands = [(i, j) for j in range(4, 64, 7) for i in range(3, 64, 5)]
+    O, centres = stable_centres(R, cands, 24, 1e-8)
+    assert len(centres) >= 12
+    seen = set()
+    for x, y in centres:
+        rec, term, nc = check_against_oracle(grrt, R, O, x, y)
+        hits = [r for r in rec if r["kind"] == grrt.DEBUG_THIN_HIT]
+        assert len(hits) == nc
+        # the END colour is the sum of the recorded crossings' emission
+        tot = np.zeros(3)
+        for h in hits:
+            tot += np.array(h["v"][1:4])
+        np.testing.assert_array_equal(tot, rec[-1]["v"][3:6])
+        steps = [r for r in rec if r["kind"] == grrt.DEBUG_STEP]
+        assert all(math.isnan(r["v"][4]) and math.isnan(r["v"][5]) for r in steps)
+        assert not any(r["kind"] in (grrt.DEBUG_MARCH_ENTRY, grrt.DEBUG_MARCH_EXIT) for r in rec)
+        seen.add((int(term), int(nc) > 0))
+    # the sample set covers the horizon, a lit escape and a dark escape
+    assert any(t == 0 for t, _ in seen) and (1, True) in seen and (1, False) in seen, seen
+
+
+def test_debug_trace_volumetric(grrt, need_gpu):
+    freqs = grrt.log_bins(1e14, 1e18, 32)
+    R = grrt.Renderer(grrt.config_params(3, width=48, height=48), freqs=freqs)
+    cands = [(i, j) for j in range(1, 48, 2) for i in range(0, 48, 2)]
+    # the volumetric RGB colour is rounding-sensitive: strict and FMA oracle
+    # builds agree to 1e-8 on 3 of 40 marching centres here, to 1e-7 on 6
+    O, centres = stable_centres(R, cands, 16, 1e-7)
+    assert len(centres) >= 8
+    marched = 0
+    for x, y in centres:
+        rec, term, nc = check_against_oracle(grrt, R, O, x, y)
+        entries = [r for r in rec if r["kind"] == grrt.DEBUG_MARCH_ENTRY]
+        exits = [r for r in rec if r["kind"] == grrt.DEBUG_MARCH_EXIT]
+        assert len(entries) == len(exits) == nc
+        for r in rec:
+            if r["kind"] == grrt.DEBUG_STEP:
+                assert r["v"][4] > 0 and r["v"][5] > 0
+                assert 0 <= r["event"] <= 3
+        if exits:
+            marched += 1
+            # the last exit's running colour is the END colour (no sky)
+            np.testing.assert_array_equal(exits[-1]["v"][:3], rec[-1]["v"][3:6])
+            assert all(e["aux"] >= 1 for e in exits)
+    assert marched >= 3
+
+
+def test_debug_trace_truncated_keeps_end(grrt, need_gpu):
+    R = grrt.Renderer(grrt.config_params(2, width=32, height=32, background_type=0))
+    full = R.debug_trace(16.5, 10.5)
+    assert len(full) > 6
+    part = R.debug_trace(16.5, 10.5, capacity=4)
+    assert len(part) == 4
+    for a, b in zip(part, full[:3] + [full[-1]]):
+        assert (a["kind"], a["step"], a["event"], a["aux"]) == (b["kind"], b["step"], b["event"], b["aux"])
+        np.testing.assert_array_equal(a["v"], b["v"])
+
+
+def test_debug_pixel_prints_the_trace(grrt, need_gpu, capfd):
+    R = grrt.Renderer(grrt.config_params(2, width=32, height=32, background_type=0))
+    rec = R.debug_trace(16.5, 10.5)
+    R.debug_pixel(16, 10)
+    out = capfd.readouterr().out.splitlines()
+    out = out[out.index("Debugging pixel (16, 10) in 32x32 image"):]
+    assert out[1] == "=== DEBUG PIXEL TRACE ==="
+    assert out[2].startswith("  r0=") and out[3].startswith("  p0=(")
+    assert out[4].split() == ["step", "r", "theta", "z", "dlambda", "H", "zm", "event"]
+    n_steps = sum(1 for r in rec if r["kind"] == grrt.DEBUG_STEP)
+    rows = [ln for ln in out[6:] if ln[:1].isdigit() and len(ln.split()) >= 7]
+    assert len(rows) == n_steps
+    end = rec[-1]
+    label = {0: "-> HORIZON", 1: "-> ESCAPED", 2: "-> MAX STEPS"}[end["event"]]
+    assert any(label in ln for ln in out)
