@@ -765,7 +765,7 @@ def main():
         cpu = None
         if not args.no_cpu_baseline and world == 1:  # the CPU baseline is taken at N = 1 only
             try:
-                rays, secs, threads, kind, rows = cpu_reference_sample(0, 16)
+                rays, secs, threads, kind, _n_rows = cpu_reference_sample(0, 16)
                 cpu = {"value": rays / secs, "unit": "rays/s", "cores": threads, "kind": "reference",
                        "sample": f"rows 0,16,...,1008 of the 1024x1024 4-spp frame ({rays} rays), reference "
                                  f"src/*.cpp ({kind} build) via oracle/_ref, OpenMP, {secs:.2f} s"}

@@ -110,54 +110,90 @@ GRRT_HD Vec5<float> mixed_k1(float M, float a, float pt, float pph, const Vec5<d
     return kerr_rhs<float>(M, a, pt, pph, yf);
 }
 
+// Packed FP32 pairs: sm_100's two-wide FP32 fused multiply-add and multiply,
+// one instruction for two lanes, each lane rounded as fmaf / the float
+// product (elsewhere the lanes are computed one by one, with the same results).
+GRRT_HD float2 pk(float x, float y) { return make_float2(x, y); }
+GRRT_HD float2 pk_fma(float2 a, float2 b, float2 c) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    return __ffma2_rn(a, b, c);
+#else
+    return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+GRRT_HD float2 pk_mul(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    return __fmul2_rn(a, b);
+#else
+    return make_float2(a.x * b.x, a.y * b.y);
+#endif
+}
+
+// A 5-vector as two packed pairs (r, theta), (phi, p_r) and p_theta alone.
+struct Pk5 {
+    float2 a, b;
+    float c;
+};
+GRRT_HD Pk5 pack5(const Vec5<float>& v) { return Pk5{pk(v.r, v.th), pk(v.ph, v.pr), v.pth}; }
+GRRT_HD Vec5<float> unpack5(const Pk5& v) { return Vec5<float>{v.a.x, v.a.y, v.b.x, v.b.y, v.c}; }
+// c * v, and c * v + w, per component
+GRRT_HD Pk5 pk5_mul(float c, const Pk5& v) {
+    const float2 cc = pk(c, c);
+    return Pk5{pk_mul(cc, v.a), pk_mul(cc, v.b), c * v.c};
+}
+GRRT_HD Pk5 pk5_fma(float c, const Pk5& v, const Pk5& w) {
+    const float2 cc = pk(c, c);
+    return Pk5{pk_fma(cc, v.a, w.a), pk_fma(cc, v.b, w.b), fmaf(c, v.c, w.c)};
+}
+
 // Mixed-precision attempt: the seven right-hand sides and the stage sums in
 // FP32, the state and its update in FP64 (y5 = y + double(h * sum b_i k_i)),
 // so round-off does not accumulate along the ray. The error norm is formed in
 // FP32; its noise floor (about 1e-7 of |h k|/|y|) is why FP32 steps are
-// controlled against their own tolerance (DevScene::tol_fp32).
+// controlled against their own tolerance (DevScene::tol_fp32). The stage sums
+// run on packed pairs (three lanes of work for five components): each stage
+// state is y + h * (sum_j a_sj k_j), the sum accumulated in the tableau's
+// order with fused multiply-adds.
 // k1 = mixed_k1(y) is given by the caller (the previous accepted attempt's
 // k7, which is f at float(y5) = float(new y), or the rejected attempt's k1).
 GRRT_HD double mixed_attempt_k1(float M, float a, float pt, float pph, const Vec5<double>& y, double dl,
-                                const Vec5<float>& k1, Vec5<double>& y5, Vec5<float>& k7_out) {
+                                const Vec5<float>& k1v, Vec5<double>& y5, Vec5<float>& k7_out) {
     using namespace dp;
-    const Vec5<float> yf{static_cast<float>(y.r), static_cast<float>(y.th), static_cast<float>(y.ph),
-                         static_cast<float>(y.pr), static_cast<float>(y.pth)};
+    const Pk5 Y = pack5(Vec5<float>{static_cast<float>(y.r), static_cast<float>(y.th), static_cast<float>(y.ph),
+                                    static_cast<float>(y.pr), static_cast<float>(y.pth)});
     const float h = static_cast<float>(dl);
-#define GRRT_F(expr_r, expr_th, expr_ph, expr_pr, expr_pth) Vec5<float>{expr_r, expr_th, expr_ph, expr_pr, expr_pth}
-#define GRRT_ST(f, comb) yf.f + h * (comb)
-#define GRRT_C2(f) float(a21) * k1.f
-    const Vec5<float> k2 = kerr_rhs<float>(M, a, pt, pph, GRRT_F(GRRT_ST(r, GRRT_C2(r)), GRRT_ST(th, GRRT_C2(th)), GRRT_ST(ph, GRRT_C2(ph)), GRRT_ST(pr, GRRT_C2(pr)), GRRT_ST(pth, GRRT_C2(pth))));
-#define GRRT_C3(f) float(a31) * k1.f + float(a32) * k2.f
-    const Vec5<float> k3 = kerr_rhs<float>(M, a, pt, pph, GRRT_F(GRRT_ST(r, GRRT_C3(r)), GRRT_ST(th, GRRT_C3(th)), GRRT_ST(ph, GRRT_C3(ph)), GRRT_ST(pr, GRRT_C3(pr)), GRRT_ST(pth, GRRT_C3(pth))));
-#define GRRT_C4(f) float(a41) * k1.f + float(a42) * k2.f + float(a43) * k3.f
-    const Vec5<float> k4 = kerr_rhs<float>(M, a, pt, pph, GRRT_F(GRRT_ST(r, GRRT_C4(r)), GRRT_ST(th, GRRT_C4(th)), GRRT_ST(ph, GRRT_C4(ph)), GRRT_ST(pr, GRRT_C4(pr)), GRRT_ST(pth, GRRT_C4(pth))));
-#define GRRT_C5(f) float(a51) * k1.f + float(a52) * k2.f + float(a53) * k3.f + float(a54) * k4.f
-    const Vec5<float> k5 = kerr_rhs<float>(M, a, pt, pph, GRRT_F(GRRT_ST(r, GRRT_C5(r)), GRRT_ST(th, GRRT_C5(th)), GRRT_ST(ph, GRRT_C5(ph)), GRRT_ST(pr, GRRT_C5(pr)), GRRT_ST(pth, GRRT_C5(pth))));
-#define GRRT_C6(f) float(a61) * k1.f + float(a62) * k2.f + float(a63) * k3.f + float(a64) * k4.f + float(a65) * k5.f
-    const Vec5<float> k6 = kerr_rhs<float>(M, a, pt, pph, GRRT_F(GRRT_ST(r, GRRT_C6(r)), GRRT_ST(th, GRRT_C6(th)), GRRT_ST(ph, GRRT_C6(ph)), GRRT_ST(pr, GRRT_C6(pr)), GRRT_ST(pth, GRRT_C6(pth))));
-#define GRRT_INC(f) h * (float(b1) * k1.f + float(b3) * k3.f + float(b4) * k4.f + float(b5) * k5.f + float(b6) * k6.f)
-    y5 = Vec5<double>{y.r + double(GRRT_INC(r)), y.th + double(GRRT_INC(th)), y.ph + double(GRRT_INC(ph)),
-                      y.pr + double(GRRT_INC(pr)), y.pth + double(GRRT_INC(pth))};
-#define GRRT_E6F(f) (float(e1) * k1.f + float(e3) * k3.f + float(e4) * k4.f + float(e5) * k5.f + float(e6) * k6.f)
-    const Vec5<float> e{GRRT_E6F(r), GRRT_E6F(th), GRRT_E6F(ph), GRRT_E6F(pr), GRRT_E6F(pth)};
-#undef GRRT_F
-#undef GRRT_ST
-#undef GRRT_C2
-#undef GRRT_C3
-#undef GRRT_C4
-#undef GRRT_C5
-#undef GRRT_C6
-#undef GRRT_INC
-#undef GRRT_E6F
+    // y + h * s
+    auto stage = [&](const Pk5& sum) { return unpack5(pk5_fma(h, sum, Y)); };
+    const Pk5 K1 = pack5(k1v);
+    const Pk5 K2 = pack5(kerr_rhs<float>(M, a, pt, pph, stage(pk5_mul(float(a21), K1))));
+    const Pk5 K3 = pack5(kerr_rhs<float>(M, a, pt, pph, stage(pk5_fma(float(a32), K2, pk5_mul(float(a31), K1)))));
+    const Pk5 K4 = pack5(kerr_rhs<float>(
+        M, a, pt, pph, stage(pk5_fma(float(a43), K3, pk5_fma(float(a42), K2, pk5_mul(float(a41), K1))))));
+    const Pk5 K5 = pack5(kerr_rhs<float>(
+        M, a, pt, pph,
+        stage(pk5_fma(float(a54), K4, pk5_fma(float(a53), K3, pk5_fma(float(a52), K2, pk5_mul(float(a51), K1)))))));
+    const Pk5 K6 = pack5(kerr_rhs<float>(
+        M, a, pt, pph,
+        stage(pk5_fma(float(a65), K5,
+                      pk5_fma(float(a64), K4,
+                              pk5_fma(float(a63), K3, pk5_fma(float(a62), K2, pk5_mul(float(a61), K1))))))));
+    const Pk5 B = pk5_fma(float(b6), K6,
+                          pk5_fma(float(b5), K5, pk5_fma(float(b4), K4, pk5_fma(float(b3), K3, pk5_mul(float(b1), K1)))));
+    const Pk5 I = Pk5{pk_mul(pk(h, h), B.a), pk_mul(pk(h, h), B.b), h * B.c};
+    y5 = Vec5<double>{y.r + double(I.a.x), y.th + double(I.a.y), y.ph + double(I.b.x), y.pr + double(I.b.y),
+                      y.pth + double(I.c)};
+    const Pk5 E = pk5_fma(float(e6), K6,
+                          pk5_fma(float(e5), K5, pk5_fma(float(e4), K4, pk5_fma(float(e3), K3, pk5_mul(float(e1), K1)))));
     const Vec5<float> y5f{static_cast<float>(y5.r), static_cast<float>(y5.th), static_cast<float>(y5.ph),
                           static_cast<float>(y5.pr), static_cast<float>(y5.pth)};
     const Vec5<float> k7 = kerr_rhs<float>(M, a, pt, pph, y5f);
     k7_out = k7;
+    const Vec5<float> ev = unpack5(pk5_fma(float(e7), pack5(k7), E));
     float err = 0.0f;
-#define GRRT_ERRF(f)                                                                     \
-    {                                                                                    \
-        const float v = fabsf(h * (e.f + float(e7) * k7.f)) * recip(fabsf(y5f.f) + 1e-10f); \
-        err = (err < v) ? v : err;                                                       \
+#define GRRT_ERRF(f)                                                       \
+    {                                                                      \
+        const float v = fabsf(h * ev.f) * recip(fabsf(y5f.f) + 1e-10f);    \
+        err = (err < v) ? v : err;                                         \
     }
     GRRT_ERRF(r) GRRT_ERRF(th) GRRT_ERRF(ph) GRRT_ERRF(pr) GRRT_ERRF(pth)
 #undef GRRT_ERRF
