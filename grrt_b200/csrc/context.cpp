@@ -287,9 +287,20 @@ bool GRRTContext::ensure_device() {
     return true;
 }
 
+// Radius inside which the mixed forms' speculation treats a long sweep as a
+// near-critical orbit: r_factor x r_horizon, and at least 1.25 x the outermost
+// photon orbit (the retrograde equatorial one, 2M (1 + cos(2/3 acos(|a|/M))):
+// 3M at a = 0, 4M at |a| = M), so that near-critical orbits of every spin lie
+// inside it (3 r_horizon is only 3.19M at a = 0.998).
+double GRRTContext::mixed_r_near() const {
+    const double x = std::min(std::fabs(spin_a) / mass, 1.0);
+    const double r_ph = 2.0 * mass * (1.0 + std::cos(2.0 / 3.0 * std::acos(x)));
+    return std::max(mixed_r_factor * r_horizon, 1.25 * r_ph);
+}
+
 DevScene GRRTContext::scene_for_launch() const {
     DevScene S = dev;
-    S.r_near_mixed = mixed_r_factor * r_horizon;
+    S.r_near_mixed = mixed_r_near();
     S.tol_fp32 = tol_fp32;
     S.mixed_margin = mixed_margin;
     return S;
@@ -351,7 +362,7 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
         e = launch_volume_rgb(S, tile, out, res, s);
     else if (mixed_thin)
         e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
-                              mixed_r_factor * r_horizon, ev_phase, s);
+                              mixed_r_near(), ev_phase, s);
     else
         e = launch_thin(S, tile, out, res, s);
     cudaEventRecord(ev1, s);

@@ -35,7 +35,7 @@ struct GRRTContext {
     // Precision form and its knobs.
     int form = GRRT_FORM_FP64;
     double mixed_r_factor = 3.0;
-    double tol_fp32 = 1e-6;
+    double tol_fp32 = 3e-6;
     double mixed_margin = 0.05;  // disk-radius margin (M) of the mixed form's re-trace test
     double vol_reach_z = 0.0;    // volumetric: max over r of z_max + 6 H (the mixed form's speculation bound)
 
@@ -77,6 +77,7 @@ struct GRRTContext {
     void build(const GRRTParams& p);
     bool ensure_device();
     grrt_b200::DevScene scene_for_launch() const;
+    double mixed_r_near() const;
 
     int render_rgb_device(const grrt_b200::DevTile& tile, float* d_rgba, double* d_rgb64, unsigned* d_fate,
                           cudaStream_t s, bool reset_stats);

@@ -180,9 +180,9 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                 step = 0;
                 k1_ok = false;
                 if (kBatch)
-                    trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.r_near_mixed);
+                    trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.r_near_mixed, S.a, pt, pph, y.th);
                 else
-                    trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near);
+                    trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near, S.a, pt, pph, y.th);
                 // Black sky: a ray whose smallest radius (closed form, from its
                 // constants of motion) lies outside the disk, r_near and every
                 // photon orbit escapes with colour 0 and no crossing.
@@ -217,7 +217,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
             const StepDecision d = pi_control(err, S.tol_fp32, dl, retry, y5.r);
             if (d.accept) {
                 ++n_acc;
-                retrace = trk.step(y, y5);
+                retrace = trk.step(y, y5, dl);
                 y = y5;
                 k1 = k7;
                 dl = d.next;

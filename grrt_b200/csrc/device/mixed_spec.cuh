@@ -10,12 +10,17 @@
 // the FP64 step sequence could make non-zero or move:
 //   - an equatorial crossing with interpolated radius in [r_in - m, r_out + m]
 //     widened by kCrossStepFrac of the step's radial extent (the interpolated
-//     radius moves with the step placement: chord error);
+//     radius moves with the step placement: chord error), or, when the step
+//     holds a radial turning point, any overlap of the step's radii with that
+//     band;
 //   - an accepted step over those radii closer than kGrazeAbs to the plane, or
 //     a theta turning point there closer than kGrazeTurn (a graze, which the
 //     FP64 steps may turn into a crossing or step over);
 //   - more than kSweptMax radians swept inside r_near (near-critical orbits:
-//     trajectory differences grow about e-fold per radian there);
+//     trajectory differences grow about e-fold per radian there; r_near covers
+//     every photon orbit);
+//   - a step ending within kPoleSin (|sin theta|) of a pole or stepping across
+//     one, where the FP32 right-hand side is not accurate enough;
 //   - the step budget;
 //   - an escape whose star lookup could find a star (see EscapeArc).
 #pragma once
@@ -36,6 +41,7 @@ constexpr double kCrossStepFrac = 0.2;
 constexpr double kGrazeAbs = 2e-3;
 constexpr double kGrazeTurn = 0.1;
 constexpr double kSweptMax = 3.0;
+constexpr float kPoleSin = 0.02f;
 constexpr double kPi = 3.14159265358979323846;
 
 // sample_fate value of an escape whose star test is still to run.
@@ -59,17 +65,39 @@ struct Tracker {
     double lo = 0.0, hi = 0.0, r_near = 0.0;
     bool disk = false;
     double swept = 0.0;
+    double a2e2 = 0.0, l2 = 0.0;  // a^2 p_t^2 and p_phi^2 of the ray
+    float sin_th = 0.0f;          // FP32 sin(theta) of the current state
 
-    GRRT_HD void reset(bool disk_on, double r_in, double r_out, double margin, double r_near_) {
+    // th0: the ray's initial theta.
+    GRRT_HD void reset(bool disk_on, double r_in, double r_out, double margin, double r_near_, double a, double pt,
+                       double pph, double th0) {
         disk = disk_on;
         lo = r_in - margin;
         hi = r_out + margin;
         r_near = r_near_;
         swept = 0.0;
+        a2e2 = a * a * pt * pt;
+        l2 = pph * pph;
+        float c0;
+        fast_sincos(static_cast<float>(th0), sin_th, c0);
     }
 
-    // One accepted step y -> y5; true when the sample needs the FP64 re-trace.
-    GRRT_HD bool step(const Vec5<double>& y, const Vec5<double>& y5) {
+    // cos^2 of the colatitude where the theta motion turns, from the Carter
+    // constant Q = p_theta^2 + cos^2(theta) (p_phi^2 / sin^2(theta) - a^2 p_t^2)
+    // at a state with sin, cos of theta (s, c): the root u in [0, 1] of
+    // a^2 p_t^2 u^2 + (Q + p_phi^2 - a^2 p_t^2) u - Q = 0.
+    GRRT_HD double turning_cos2(double pth, double s, double c) const {
+        const double s2 = fmax(s * s, 1e-30), c2 = c * c;
+        const double Q = fmax(pth * pth + c2 * (l2 / s2 - a2e2), 0.0);
+        const double B = Q + l2 - a2e2;
+        if (a2e2 <= 0.0) return (Q + l2 > 0.0) ? Q / (Q + l2) : 0.0;
+        const double disc = sqrt(B * B + 4.0 * a2e2 * Q);
+        return (B >= 0.0) ? 2.0 * Q / (B + disc) : (disc - B) / (2.0 * a2e2);
+    }
+
+    // One accepted step y -> y5 of affine length h; true when the sample
+    // needs the FP64 re-trace.
+    GRRT_HD bool step(const Vec5<double>& y, const Vec5<double>& y5, double h) {
         bool hit = false;
         if (disk) {
             const double d_prev = y.th - 0.5 * kPi, d_new = y5.th - 0.5 * kPi;
@@ -77,15 +105,39 @@ struct Tracker {
                 const double rc = y.r + (-d_prev / (d_new - d_prev)) * (y5.r - y.r);
                 const double w = kCrossStepFrac * fabs(y5.r - y.r);
                 hit = rc >= lo - w && rc <= hi + w;
+                // A radial turning point inside the step (p_r changes sign):
+                // r is then far from linear in theta and the chord can miss
+                // the crossing radius by most of the step's radial extent. The
+                // radii along the step lie in [min r - dip, max r], with
+                // dip <= h min|p_r| / 2 for a quadratic r(lambda) with
+                // dr/dlambda = (Delta / Sigma) p_r and Delta / Sigma <= 1
+                // (taken twice for the higher terms); an overlap with the band
+                // counts.
+                if (!hit && y.pr * y5.pr <= 0.0) {
+                    const double dip = fabs(h) * fmin(fabs(y.pr), fabs(y5.pr));
+                    hit = fmin(y.r, y5.r) - dip <= hi + w && fmax(y.r, y5.r) >= lo - w;
+                }
             } else if (y5.r >= lo && y5.r <= hi) {
                 const double m = fmin(fabs(d_prev), fabs(d_new));
                 hit = m < kGrazeAbs || (y.pth * y5.pth <= 0.0 && m < kGrazeTurn);
             }
         }
+        // Near a pole the right-hand side's 1/sin(theta) terms amplify the
+        // FP32 sine's absolute error (about 1e-7) into the trajectory; a ray
+        // that ends a step within kPoleSin of the axis, steps across it
+        // (sin(theta) changes sign), or turns in theta inside a step closer to
+        // it than kPoleSin (the turning colatitude from the Carter constant:
+        // a long step can pass the pole between its ends) is re-traced.
+        const float s0 = sin_th;  // sin(theta) at y, from the previous step
+        float s5, c5;
+        fast_sincos(static_cast<float>(y5.th), s5, c5);
+        sin_th = s5;
+        if (fabsf(s5) < kPoleSin || s0 * s5 <= 0.0f) hit = true;
+        if (!hit && y.pth * y5.pth <= 0.0 &&
+            1.0 - turning_cos2(y5.pth, s5, c5) < static_cast<double>(kPoleSin) * kPoleSin)
+            hit = true;
         if (y.r < r_near) {
-            float s, c;
-            fast_sincos(static_cast<float>(y.th), s, c);
-            swept += fabs(y5.th - y.th) + fabs(y5.ph - y.ph) * static_cast<double>(fabsf(s));
+            swept += fabs(y5.th - y.th) + fabs(y5.ph - y.ph) * static_cast<double>(fabsf(s0));
             if (swept > kSweptMax) hit = true;
         }
         return hit;

@@ -81,12 +81,13 @@ struct DevScene {
     DevVolume vol;
 
     // mixed forms (speculative FP32 pass, then FP64 re-trace): the FP32
-    // tolerance; r_near_mixed = r_factor x r_horizon, inside which a
+    // tolerance; r_near_mixed = max(r_factor x r_horizon, 1.25 x the outermost
+    // photon orbit radius), inside which a
     // near-critical sweep sends a sample to the re-trace (and beyond which,
     // on a black sky, a certain escape is final); mixed_margin, the disk-radius
     // margin of the re-trace test
     double r_near_mixed = 0;
-    double tol_fp32 = 1e-6;
+    double tol_fp32 = 3e-6;
     double mixed_margin = 0.05;
 };
 

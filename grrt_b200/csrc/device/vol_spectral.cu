@@ -492,7 +492,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
-                trk.reset(false, 0.0, 0.0, 0.0, S.r_near_mixed);
+                trk.reset(false, 0.0, 0.0, 0.0, S.r_near_mixed, S.a, pt, pph, y.th);
                 k1_ok = false;
                 live = true;
             }
@@ -521,7 +521,7 @@ vol_speculate_kernel(const __grid_constant__ DevScene S, const DevTile tile, con
             const StepDecision d = pi_control(err, S.tol_fp32, dl, retry, y5.r);
             if (d.accept) {
                 ++cnt.accepted;
-                retrace = vol_reach(reach, rr, y, y5) || trk.step(y, y5);
+                retrace = vol_reach(reach, rr, y, y5) || trk.step(y, y5, dl);
                 y = y5;
                 k1 = k7;
                 dl = d.next;

@@ -505,7 +505,7 @@ struct GRRTSurrogate {
         }
         if (!ensure_inference(std::min(n, kChunk))) return false;
         DevMixedBuffers mb = mixed_buffers_with_list(ctx->d_mixed_scratch, n, ctx->d_queue);
-        mb.r_near = ctx->mixed_r_factor * ctx->r_horizon;
+        mb.r_near = ctx->mixed_r_near();
         mb.margin = ctx->mixed_margin;
         // the surrogate's kernels run on its own stream, ordered after the caller's
         cudaEvent_t e_in = nullptr;

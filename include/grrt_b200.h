@@ -56,10 +56,11 @@ GRRT_EXPORT int grrt_get_precision(const GRRTContext* ctx);
 
 /* Mixed-form knobs. Thin disk: every sample is first integrated with FP32
  * right-hand sides against tol_fp32; a sample that sweeps more than 3 rad
- * inside r_factor * r_horizon (near-critical) is among those re-traced in FP64.
- * Volumetric disk: outer steps that start at r > r_factor * r_horizon use FP32
- * right-hand sides against tol_fp32. Defaults 3.0 and 1e-6; r_factor must lie
- * in [1, 100] and tol_fp32 in [1e-9, 1e-2], else -1. */
+ * inside r_near = max(r_factor * r_horizon, 1.25 x the outermost photon orbit)
+ * (near-critical) is among those re-traced in FP64. Volumetric disk: the same
+ * speculation, with the volume's reach in place of the disk test. Defaults 3.0
+ * and 3e-6; r_factor must lie in [1, 100] and tol_fp32 in [1e-9, 1e-2], else
+ * -1. */
 GRRT_EXPORT int grrt_set_mixed_params(GRRTContext* ctx, double r_factor, double tol_fp32);
 
 /* Device time (ms, CUDA events on the render stream) of each kernel phase of

@@ -47,7 +47,7 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
     double dl = dl0;
     int retry = 0, step = 0;
     mixed::Tracker trk;
-    trk.reset(disk_on, sc[7], sc[8], sc[9], sc[10]);
+    trk.reset(disk_on, sc[7], sc[8], sc[9], sc[10], a, pt, pph, y.th);
     Vec5<float> k7{};
     *term_out = -1;
     // black sky: a ray whose closed-form smallest radius lies outside the disk,
@@ -70,7 +70,7 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
         const double err = mixed_attempt_impl(float(M), float(a), float(pt), float(pph), y, dl, y5, k7);
         const StepDecision d = pi_control(err, tol32, dl, retry, y5.r);
         if (d.accept) {
-            const bool hit = trk.step(y, y5);
+            const bool hit = trk.step(y, y5, dl);
             y = y5;
             if (hit) return 1;
             dl = d.next;

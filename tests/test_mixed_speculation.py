@@ -20,13 +20,16 @@ from test_device_math import devmath  # noqa: F401  (fixture)
 STAR_TOL = 0.003  # the star catalogue's angular tolerance (rad)
 
 
-def speculate_all(L, R, px, py, margin=0.05, r_factor=3.0, tol32=1e-6):
+def speculate_all(L, R, px, py, margin=0.05, r_factor=3.0, tol32=3e-6):
     sc = R.table("scalars")
     M, a, rh, isco, robs, _tol, max_steps = sc[:7]
     disk = R.values["disk_enabled"] != 0
     r_in, r_out = (R.table("flux_meta")[1], R.table("flux_meta")[2]) if disk else (0.0, 0.0)
     stars = R.values["background_type"] == 1
-    v = np.array([M, a, rh + 0.01, 1000.0, 0.01 * robs, tol32, max_steps, r_in, r_out, margin, r_factor * rh,
+    # near-critical radius: r_factor r_h, at least 1.25 x the outermost photon orbit (as the library)
+    r_ph = 2.0 * M * (1.0 + math.cos(2.0 / 3.0 * math.acos(min(abs(a) / M, 1.0))))
+    r_near = max(r_factor * rh, 1.25 * r_ph)
+    v = np.array([M, a, rh + 0.01, 1000.0, 0.01 * robs, tol32, max_steps, r_in, r_out, margin, r_near,
                   1.0 if disk else 0.0, 1.0 if stars else 0.0])
     PD, PI = C.POINTER(C.c_double), C.POINTER(C.c_int)
     hold = []
