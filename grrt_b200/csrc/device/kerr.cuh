@@ -22,13 +22,10 @@
 #include <cmath>
 
 #define GRRT_HD __host__ __device__ __forceinline__
-// The right-hand side is inlined at its seven call sites per attempt unless
-// GRRT_RHS_CALL is set (one shared body: less code, a call per evaluation).
-#ifdef GRRT_RHS_CALL
-#define GRRT_RHS_ATTR __host__ __device__ __noinline__
-#else
-#define GRRT_RHS_ATTR GRRT_HD
-#endif
+// The right-hand side is inlined at its call sites (seven per attempt) unless
+// the translation unit sets GRRT_RHS_CALL_F64, which makes the FP64 one a
+// call to one shared body (less code to fetch, a call per evaluation). The
+// FP32 one stays inlined: its kernels are issue-bound and lose to the calls.
 
 namespace grrt_b200 {
 
@@ -126,7 +123,7 @@ GRRT_HD float recip(float x) {
 // Returns dx/dlambda and dp/dlambda for (r, theta, phi, p_r, p_theta) given the
 // constants p_t, p_phi.
 template <typename T>
-GRRT_RHS_ATTR Vec5<T> kerr_rhs(T M, T a, T pt, T pph, const Vec5<T>& y) {
+GRRT_HD Vec5<T> kerr_rhs_body(T M, T a, T pt, T pph, const Vec5<T>& y) {
     using std::fabs;
     const T r = y.r, pr = y.pr, pth = y.pth;
     T s, c;
@@ -156,6 +153,22 @@ GRRT_RHS_ATTR Vec5<T> kerr_rhs(T M, T a, T pt, T pph, const Vec5<T>& y) {
     const T dpr = H * T(2) * r * iS - dF * hiS;
     const T dpth = -(dG * hiS + H * T(2) * a2 * s * c * iS);
     return Vec5<T>{dr, dth, dph, dpr, dpth};
+}
+
+#ifdef GRRT_RHS_CALL_F64
+static __host__ __device__ __noinline__ Vec5<double> kerr_rhs_f64_call(double M, double a, double pt, double pph,
+                                                                       const Vec5<double>& y) {
+    return kerr_rhs_body<double>(M, a, pt, pph, y);
+}
+#endif
+
+template <typename T>
+GRRT_HD Vec5<T> kerr_rhs(T M, T a, T pt, T pph, const Vec5<T>& y) {
+#ifdef GRRT_RHS_CALL_F64
+    if constexpr (sizeof(T) == sizeof(double)) return kerr_rhs_f64_call(M, a, pt, pph, y);
+    else
+#endif
+        return kerr_rhs_body<T>(M, a, pt, pph, y);
 }
 
 }  // namespace grrt_b200

@@ -27,11 +27,10 @@
 // The rest are listed and re-traced from the camera by the FP64 kernel; a
 // resolve pass sums each pixel's samples in order.
 // The volumetric kernels end on a few long rays, one warp per SM, where
-// instruction fetch stalls as much as arithmetic: one shared body of the
+// instruction fetch stalls as much as arithmetic: one shared body of the FP64
 // right-hand side instead of twelve inlined copies (Kerr a=0.9, 512x512, 32
-// bins: 82 -> 74-79 ms for the FP64 form, 85 -> 80 ms for the mixed form on
-// B200).
-#define GRRT_RHS_CALL 1
+// bins: 82 -> 74-79 ms for the FP64 form on B200).
+#define GRRT_RHS_CALL_F64 1
 #include <cuda_runtime.h>
 
 #include <cstdint>
