@@ -374,6 +374,18 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
                 retry = 0;
                 ++step;
                 term = start_test(S, step, y.r);
+                // Black sky: once the escape is certain (outgoing beyond the
+                // disk, r_near and every photon orbit, far from the step
+                // budget) no crossing can follow and no star is looked up, so
+                // the colour, the crossings and the fate are those the FP64
+                // trace to r_escape would give.
+                if (term < 0 && !S.stars_on) {
+                    const double m = kBatch ? S.mixed_margin : mb.margin;
+                    const double r_near = kBatch ? S.r_near_mixed : mb.r_near;
+                    const double r_min = fmax(fmax(mixed::kEscapeRMin * S.M, r_near),
+                                              S.disk_on ? S.r_out + 2.0 * m : 0.0);
+                    if (mixed::certain_escape(y, r_min, step, S.max_steps)) term = kTermEscaped;
+                }
             } else {
                 dl = d.next;
                 ++retry;
