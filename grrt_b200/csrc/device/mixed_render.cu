@@ -147,8 +147,12 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 // over one sample space, so one launch per phase covers all cameras.
 // Inside, S names the scene of the lane's current sample.
 
+// Five resident blocks per SM (at most 96 registers): the issue-bound FP32
+// pass gains more from the fifth block's warps than it loses to the few
+// spilled registers (four blocks: 8.8 ms, five: 8.2 ms on the 1024x1024 4-spp
+// frame on B200; six, with more spills, no better).
 template <bool kBatch>
-__global__ void __launch_bounds__(kMixThreads, 4)
+__global__ void __launch_bounds__(kMixThreads, 5)
 mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
                        DevMixedBuffers mb, DevStats* stats) {
     const DevScene* sp = nullptr;
