@@ -202,8 +202,8 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                     const double r_near = kBatch ? S.r_near_mixed : mb.r_near;
                     const double r_gate =
                         fmax(fmax(mixed::kEscapeRMin * S.M, r_near), S.disk_on ? S.r_out + 2.0 * m : 0.0);
-                    settled = surr::camera_ray_min_radius(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p) >
-                              r_gate;
+                    settled =
+                        surr::camera_ray_clears(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p, r_gate);
                 }
                 live = true;
             }

@@ -524,7 +524,7 @@ __global__ void prepare_kernel(const __grid_constant__ DevScene S, const DevTile
         // black sky: never near the disk, the hole or a photon orbit (closed
         // form): colour 0 and escaped, as the FP64 method gives it
         settled = settle_radius > 0.0 &&
-                  camera_ray_min_radius(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p) > settle_radius;
+                  camera_ray_clears(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p, settle_radius);
         keep = !settled;
         if (settled) {
             mb.sample_rgb[3 * static_cast<size_t>(q) + 0] = 0.0;

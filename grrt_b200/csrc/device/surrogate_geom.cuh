@@ -131,6 +131,32 @@ GRRT_HD double camera_ray_min_radius(double M, double a, double r_h, double r_ca
     return turning_radius(M, a, constants(a, theta_cam, p), r_h, r_cam);
 }
 
+// Whether a camera ray's smallest radius exceeds r_gate (< r_cam): the same
+// answer as camera_ray_min_radius(...) > r_gate, from the same inward scan,
+// but the scan stops at r_gate and the bracket that holds r_gate is settled by
+// the sign of R at r_gate (the turning point lies above r_gate exactly when
+// r_gate is in the forbidden region) instead of by bisection.
+GRRT_HD bool camera_ray_clears(double M, double a, double r_h, double r_cam, double theta_cam, const double p[4],
+                               double r_gate) {
+    if (p[1] >= 0.0) return r_cam > r_gate;
+    const RayConstants k = constants(a, theta_cam, p);
+    constexpr int kN = 96;
+    const double lo = r_h * (1.0 + 1e-9);
+    const double q = pow(r_cam / lo, 1.0 / (kN - 1));
+    double r_prev = r_cam;
+    for (int i = 1; i < kN; ++i) {
+        const double r = (i == kN - 1) ? lo : r_prev / q;
+        if (r <= r_gate) {
+            // R >= 0 at r: any turning point lies below r <= r_gate
+            if (!(scaled_potential(M, a, k, r) < 0.0)) return false;
+            return scaled_potential(M, a, k, r_gate) < 0.0;
+        }
+        if (scaled_potential(M, a, k, r) < 0.0) return true;  // turning point in (r, r_prev), above r_gate
+        r_prev = r;
+    }
+    return false;
+}
+
 // Distance (in mu = cos theta) of the ray's theta turning point from the
 // equator: mu_+ when Q >= 0 (the ray crosses the plane and turns at +-mu_+),
 // mu_- when Q < 0 (it stays in one hemisphere between mu_- and mu_+).

@@ -55,7 +55,7 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
     if (!stars_on) {
         const double p[4] = {y8[4], y8[5], y8[6], y8[7]};
         const double r_gate = fmax(fmax(mixed::kEscapeRMin * M, sc[10]), disk_on ? sc[8] + 2.0 * sc[9] : 0.0);
-        if (surr::camera_ray_min_radius(M, a, r_stop - 0.01, y8[1], y8[2], p) > r_gate) {
+        if (surr::camera_ray_clears(M, a, r_stop - 0.01, y8[1], y8[2], p, r_gate)) {
             *term_out = kTermEscaped;
             return 0;
         }
@@ -177,6 +177,14 @@ void devmath_ray_margins(double M, double a, double r_h, const double* y8, doubl
     const surr::RayConstants k = surr::constants(a, y8[2], p);
     out2[0] = (p[1] < 0.0) ? surr::capture_margin(M, a, k, r_h, y8[1]) : -1.0;
     out2[1] = surr::graze_margin(a, k);
+}
+
+// The black-sky gate both ways for a camera ray: out2 = (smallest radius by
+// the full scan and bisection, whether the scan stopped at r_gate clears it).
+void devmath_gate(double M, double a, double r_h, const double* y8, double r_gate, double* out2) {
+    const double p[4] = {y8[4], y8[5], y8[6], y8[7]};
+    out2[0] = surr::camera_ray_min_radius(M, a, r_h, y8[1], y8[2], p);
+    out2[1] = surr::camera_ray_clears(M, a, r_h, y8[1], y8[2], p, r_gate) ? 1.0 : 0.0;
 }
 
 // The surrogate's training trace (the FP64 method, as the thin-disk kernel)

@@ -66,3 +66,30 @@ def test_closed_form_margins(grrt, devmath, name, kw):  # noqa: F811
           f"relevant crossings after the second {int(multi.sum())} (|m| <= {worst_multi:.3f}); in critical band {np.mean(np.abs(cap) < CRITICAL_BAND):.4f}")
     assert worst_bad < 0.01 and bad.mean() < 0.005
     assert worst_multi < CRITICAL_BAND
+
+
+@pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
+def test_gate_scan_stops_at_gate_radius(grrt, devmath, name, kw):  # noqa: F811
+    """The black-sky gate (camera_ray_clears: scan stopped at r_gate, bracket
+    settled by the sign of R there) gives the same answer as comparing the
+    full scan-and-bisection smallest radius with r_gate, on every camera ray of
+    a frame and several gate radii."""
+    n = 96
+    R = grrt.Renderer(grrt.config_params(2, width=n, height=n, spp=1, background_type=0, **kw))
+    M, a, rh = R.table("scalars")[:3]
+    PD = C.POINTER(C.c_double)
+    devmath.devmath_gate.argtypes = [C.c_double, C.c_double, C.c_double, PD, C.c_double, PD]
+    px, py = jittered_samples(n, n, 1, np.arange(n * n))
+    O = Oracle(R)
+    rays = [O.camera_ray(x, y) for x, y in zip(px, py)]
+    cleared = 0
+    for r_gate in (5.0, 10.0, 20.1, 30.0):
+        for y8 in rays:
+            out = np.zeros(2)
+            devmath.devmath_gate(M, a, rh, y8.ctypes.data_as(PD), r_gate, out.ctypes.data_as(PD))
+            r_min = out[0]
+            if abs(r_min - r_gate) < 1e-9 * r_gate:
+                continue  # the root at the gate radius itself (bisection precision)
+            assert (out[1] == 1.0) == (r_min > r_gate), (name, r_gate, r_min)
+            cleared += int(out[1])
+    assert cleared > 0
