@@ -84,15 +84,24 @@ GRRT_HD T dp45_attempt_k1(T M, T a, T pt, T pph, const Vec5<T>& y, T h, const Ve
     k7_out = k7;
     // err = max |h (sum e_i k_i)| / (|y5| + 1e-10); max written as the
     // standard library's (a < b) ? b : a so a NaN term is skipped as there.
-    T err = T(0);
-#define GRRT_ERR(f)                                                            \
-    {                                                                          \
-        const T v = fabs(h * (e.f + T(e7) * k7.f)) / (fabs(y5.f) + T(1e-10)); \
-        err = (err < v) ? v : err;                                             \
+    // The largest quotient is picked by cross-multiplied comparisons
+    // (numerators >= 0, denominators > 0) and divided once: the same value as
+    // dividing each and taking the maximum, but for quotients within a rounding
+    // of each other, where either may be taken. A NaN term fails every
+    // comparison and is skipped.
+    T num = T(0), den = T(1);
+#define GRRT_ERR(f)                                            \
+    {                                                          \
+        const T n_ = fabs(h * (e.f + T(e7) * k7.f));           \
+        const T d_ = fabs(y5.f) + T(1e-10);                    \
+        if (num * d_ < n_ * den) {                             \
+            num = n_;                                          \
+            den = d_;                                          \
+        }                                                      \
     }
     GRRT_ERR(r) GRRT_ERR(th) GRRT_ERR(ph) GRRT_ERR(pr) GRRT_ERR(pth)
 #undef GRRT_ERR
-    return err;
+    return num / den;
 }
 
 // One DP45 attempt from scratch: returns the 5th-order state in y5 and the error norm.
