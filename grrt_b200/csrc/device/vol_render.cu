@@ -10,6 +10,12 @@
 // phase) or one RK4 march step (march phase); the three channels' transfer
 // state sits in registers. The list instantiation is the FP64 re-trace of the
 // mixed form (its speculation is in vol_spectral.cu).
+// One shared body of the FP64 right-hand side instead of inlined copies: the
+// launches end on a few long rays, where instruction fetch stalls (Kerr
+// a=0.9, 512x512 RGB: 49 -> 41 ms for the FP64 form on B200). The FP64 form
+// and the mixed form's re-trace are both in this file, so their arithmetic is
+// identical.
+#define GRRT_RHS_CALL_F64 1
 #include <cuda_runtime.h>
 
 #include <cstdint>
