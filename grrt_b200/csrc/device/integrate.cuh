@@ -267,4 +267,46 @@ GRRT_HD StepDecision pi_control(double err, double tol, double dl, int retry,
     return d;
 }
 
+// The FP32 pass's controller: pi_control with (tol/err)^0.2 formed from a
+// single-precision quotient (the FP32 error norm carries no more digits).
+GRRT_HD double step_factor_ratio(double tol, double err) {
+#ifdef __CUDA_ARCH__
+    return static_cast<double>(__powf(__fdividef(static_cast<float>(tol), static_cast<float>(err)), 0.2f));
+#else
+    return static_cast<double>(powf(static_cast<float>(tol) / static_cast<float>(err), 0.2f));
+#endif
+}
+
+GRRT_HD StepDecision pi_control_f32(double err, double tol, double dl, int retry,
+                                                   double r5) {
+    constexpr double safety = 0.9, grow_max = 5.0, shrink_max = 0.2, dl_min = 1e-6;
+    StepDecision d;
+    const double ar = fabs(r5);
+    const double cap = 5.0 * ((ar < 1.0) ? 1.0 : ar);
+    if (retry >= 20) {
+        d.accept = true;
+        d.next = dl;
+        return d;
+    }
+    if (err <= tol) {
+        double f = (err > 1e-30) ? safety * step_factor_ratio(tol, err) : grow_max;
+        f = (f < 1.0) ? 1.0 : (grow_max < f) ? grow_max : f;
+        const double nx = dl * f;
+        d.accept = true;
+        d.next = (cap < nx) ? cap : nx;
+        return d;
+    }
+    double f = safety * step_factor_ratio(tol, err);
+    f = (f < shrink_max) ? shrink_max : (1.0 < f) ? 1.0 : f;
+    const double ndl = dl * f;
+    if (ndl < dl_min) {
+        d.accept = true;
+        d.next = (cap < dl_min) ? cap : dl_min;
+        return d;
+    }
+    d.accept = false;
+    d.next = ndl;
+    return d;
+}
+
 }  // namespace grrt_b200

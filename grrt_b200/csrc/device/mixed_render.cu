@@ -223,7 +223,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
             const double err =
                 mixed_attempt_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, k1, y5, k7);
             ++n_att;
-            const StepDecision d = pi_control(err, S.tol_fp32, dl, retry, y5.r);
+            const StepDecision d = pi_control_f32(err, S.tol_fp32, dl, retry, y5.r);
             if (d.accept) {
                 ++n_acc;
                 retrace = trk.step(y, y5, dl);

@@ -79,7 +79,7 @@ struct Tracker {
         a2e2 = a * a * pt * pt;
         l2 = pph * pph;
         float c0;
-        fast_sincos(static_cast<float>(th0), sin_th, c0);
+        rhs_sincos(static_cast<float>(th0), sin_th, c0);
     }
 
     // cos^2 of the colatitude where the theta motion turns, from the Carter
@@ -130,7 +130,7 @@ struct Tracker {
         // a long step can pass the pole between its ends) is re-traced.
         const float s0 = sin_th;  // sin(theta) at y, from the previous step
         float s5, c5;
-        fast_sincos(static_cast<float>(y5.th), s5, c5);
+        rhs_sincos(static_cast<float>(y5.th), s5, c5);
         sin_th = s5;
         if (fabsf(s5) < kPoleSin || s0 * s5 <= 0.0f) hit = true;
         if (!hit && y.pth * y5.pth <= 0.0 &&

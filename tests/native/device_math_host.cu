@@ -68,7 +68,7 @@ int devmath_speculate(const double* sc, const double* y8, const double* st_th, c
         }
         Vec5<double> y5;
         const double err = mixed_attempt_impl(float(M), float(a), float(pt), float(pph), y, dl, y5, k7);
-        const StepDecision d = pi_control(err, tol32, dl, retry, y5.r);
+        const StepDecision d = pi_control_f32(err, tol32, dl, retry, y5.r);
         if (d.accept) {
             const bool hit = trk.step(y, y5, dl);
             y = y5;
