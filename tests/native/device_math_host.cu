@@ -31,6 +31,20 @@ double devmath_dp45(double M, double a, const double* y8, double h, double* out5
 }
 
 
+// One tracker step of the speculative pass: tr = (disk_on, r_in, r_out,
+// margin, r_near, a, p_t, p_phi), y and y5 = (r, theta, phi, p_r, p_theta),
+// h the step length. Returns 1 when the step sends the sample to the re-trace.
+// out[0] = cos^2 of the theta turning colatitude at y5 (Carter constant).
+int devmath_tracker_step(const double* tr, const double* y, const double* y5, double h, double* out) {
+    mixed::Tracker t;
+    t.reset(tr[0] != 0.0, tr[1], tr[2], tr[3], tr[4], tr[5], tr[6], tr[7], y[1]);
+    const Vec5<double> a{y[0], y[1], y[2], y[3], y[4]}, b{y5[0], y5[1], y5[2], y5[3], y5[4]};
+    float s5, c5;
+    fast_sincos(static_cast<float>(b.th), s5, c5);
+    out[0] = t.turning_cos2(b.pth, s5, c5);
+    return t.step(a, b, h) ? 1 : 0;
+}
+
 // The mixed form's speculative pass for one sample, as mixed_speculate_kernel
 // and mixed_star_kernel run it. sc = (M, a, r_stop, r_escape, dl0, tol_fp32,
 // max_steps, r_in, r_out, margin, r_near, disk_on, stars_on); star arrays may

@@ -86,3 +86,58 @@ def test_speculation_flags_every_sample_with_colour(grrt, devmath, name, cfg, n,
     frac = flags.mean()
     print(f"\n  [{name}] flagged {frac:.3f} of samples; coloured {coloured.mean():.3f}")
     assert frac <= max(0.5, 1.6 * coloured.mean())
+
+
+def tracker_step(L, tr, y, y5, h):
+    PD = C.POINTER(C.c_double)
+    L.devmath_tracker_step.restype = C.c_int
+    L.devmath_tracker_step.argtypes = [PD, PD, PD, C.c_double, PD]
+    tr, y, y5, out = (np.ascontiguousarray(v, dtype=np.float64) for v in (tr, y, y5, [0.0]))
+    hit = L.devmath_tracker_step(tr.ctypes.data_as(PD), y.ctypes.data_as(PD), y5.ctypes.data_as(PD), h,
+                                 out.ctypes.data_as(PD))
+    return hit, out[0]
+
+
+def test_tracker_polar_and_turning_rules(devmath):  # noqa: F811
+    """The speculation's polar and turning-point rules on hand-made steps
+    (mixed_spec.cuh): a step ending near a pole, a step across the axis, a
+    theta turning point closer to the axis than the threshold inside a long
+    step, and an equatorial crossing whose chord misses the disk band while
+    the step holds a radial turning point inside it. Plain steps away from
+    all of these are not flagged."""
+    L = devmath
+    half = math.pi / 2
+    # disk [2, 20], margin 0.05, r_near 5; a = 0.9, p_t = -1, p_phi = 0.1
+    tr = [1.0, 2.0, 20.0, 0.05, 5.0, 0.9, -1.0, 0.1]
+    # an ordinary step high above the plane: not flagged
+    hit, _ = tracker_step(L, tr, [40, 0.8, 0, 0.5, 0.3], [41, 0.81, 0.1, 0.5, 0.3], 1.0)
+    assert hit == 0
+    # ends within |sin theta| < 0.02 of the pole
+    hit, _ = tracker_step(L, tr, [40, 0.05, 0, 0.5, -0.3], [41, 0.01, 0.1, 0.5, -0.3], 1.0)
+    assert hit == 1
+    # steps across the axis (theta changes sign)
+    hit, _ = tracker_step(L, tr, [40, 0.05, 0, 0.5, -0.3], [41, -0.04, 0.1, 0.5, -0.3], 1.0)
+    assert hit == 1
+    # theta turns inside the step, both ends 0.1 from the axis: flagged when
+    # the Carter-constant turning point lies within 0.02 of the axis
+    hit, u = tracker_step(L, tr, [40, 0.1, 0, 0.5, -0.05], [41, 0.1, 0.1, 0.5, 0.05], 1.0)
+    assert (1.0 - u < 0.02 ** 2) == (hit == 1)
+    tr_lz = list(tr)
+    tr_lz[7] = 0.0  # zero angular momentum: the ray passes over the pole itself
+    hit, u = tracker_step(L, tr_lz, [40, 0.1, 0, 0.5, -0.05], [41, 0.1, 0.1, 0.5, 0.05], 1.0)
+    assert hit == 1 and u == pytest.approx(1.0)
+    tr_big = list(tr)
+    tr_big[7] = 40.0  # large p_phi: turns far from the axis
+    hit, u = tracker_step(L, tr_big, [40, 0.6, 0, 0.5, -0.05], [41, 0.6, 0.1, 0.5, 0.05], 1.0)
+    assert hit == 0 and 1.0 - u > 0.02 ** 2
+    # an equatorial crossing whose chord lands at 20.40, outside [1.95, 20.05]
+    # widened by 0.2 |dr| = 0.02 ...
+    y = [20.30, half - 0.01, 0, -0.02, 0.0]
+    y5 = [20.40, half + 0.01, 0.1, -0.01, 0.0]
+    hit, _ = tracker_step(L, tr, y, y5, 3.0)
+    assert hit == 0
+    # ... is flagged when p_r changes sign in the step (radial turning point:
+    # the radii dip by up to h min|p_r| below the smaller end)
+    y5_turn = [20.40, half + 0.01, 0.1, 0.2, 0.0]
+    hit, _ = tracker_step(L, tr, [20.30, half - 0.01, 0, -0.2, 0.0], y5_turn, 3.0)
+    assert hit == 1
