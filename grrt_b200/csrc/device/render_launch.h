@@ -117,6 +117,12 @@ cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const D
 cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
                                  const ThinOutputs& out, DevStats* stats, cudaStream_t stream);
 
+// Re-trace lists in sample order (list_order.cu): list[0 .. *count) holds
+// distinct sample indices below n; they are rewritten in increasing order.
+// scratch: order_list_scratch_bytes(n) bytes, 256-byte aligned.
+size_t order_list_scratch_bytes(size_t n);
+cudaError_t order_sample_list(unsigned* list, const unsigned* count, size_t n, void* scratch, cudaStream_t stream);
+
 // In-place tone mapping of a device RGBA float frame (tonemap.cu; 16-byte aligned).
 cudaError_t launch_tonemap(float* d_rgba, int width, int height, cudaStream_t stream);
 

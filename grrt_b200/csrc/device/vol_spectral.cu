@@ -661,7 +661,9 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
 size_t volume_mixed_scratch_bytes(const DevTile& tile, int g2, int nb) {
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
     // header (counters), the re-trace list (rounded up to 256 B), per-sample J
-    return 1024 + ((n * sizeof(unsigned) + 255) / 256) * 256 + n * nb * sizeof(double);
+    // (rounded up to 256 B), the list ordering's bitmap and block sums
+    return 1024 + ((n * sizeof(unsigned) + 255) / 256) * 256 + ((n * nb * sizeof(double) + 255) / 256) * 256 +
+           order_list_scratch_bytes(n);
 }
 
 cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
@@ -681,7 +683,9 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     unsigned* list_count = reinterpret_cast<unsigned*>(base + 512);
     unsigned* list = reinterpret_cast<unsigned*>(base + 1024);
     auto* sample_spec = reinterpret_cast<double*>(base + 1024 + ((n * sizeof(unsigned) + 255) / 256) * 256);
-    if (static_cast<size_t>(reinterpret_cast<unsigned char*>(sample_spec + n * nb) - base) > scratch_bytes)
+    unsigned char* order_scratch =
+        reinterpret_cast<unsigned char*>(sample_spec) + ((n * nb * sizeof(double) + 255) / 256) * 256;
+    if (static_cast<size_t>(order_scratch - base) + order_list_scratch_bytes(n) > scratch_bytes)
         return cudaErrorInvalidValue;
     int lb = sh.sms * sh.per_list;
     if (!res.spectral_scratch || res.spectral_scratch_elems < static_cast<size_t>(4) * nb * lb * kSpecThreads)
@@ -701,6 +705,8 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     vol_speculate_kernel<false><<<sb, kSpecThreads, 0, stream>>>(S, tile, reach, out.fate, res.queue, list,
                                                                 list_count, nullptr, res.stats);
     e = cudaGetLastError();
+    // the re-trace takes its samples in the FP64 form's order
+    if (e == cudaSuccess) e = order_sample_list(list, list_count, n, order_scratch, stream);
     if (e != cudaSuccess) return e;
     mark(1);
     vol_spectral_kernel<true><<<lb, kSpecThreads, 0, stream>>>(S, tile, freqs, nb, sample_spec, out.fate,
