@@ -478,8 +478,18 @@ __global__ void mixed_resolve_kernel(const __grid_constant__ DevScene S0, const 
     }
 }
 
+// Header, per-sample colour and fate, the re-trace and speculation lists, then
+// (256-byte aligned) room for ordering the re-trace list.
+static size_t mixed_order_offset(size_t n_samples) {
+    return ((n_samples * (3 * sizeof(double) + 3 * sizeof(unsigned)) + 1024 + 255) / 256) * 256;
+}
+
 size_t mixed_scratch_bytes_for(size_t n_samples) {
-    return n_samples * (3 * sizeof(double) + 3 * sizeof(unsigned)) + 1024;
+    return mixed_order_offset(n_samples) + order_list_scratch_bytes(n_samples);
+}
+
+void* mixed_order_scratch(void* scratch, size_t n_samples) {
+    return static_cast<unsigned char*>(scratch) + mixed_order_offset(n_samples);
 }
 
 size_t mixed_scratch_bytes(const DevTile& tile, int g2) {

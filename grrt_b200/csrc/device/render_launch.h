@@ -89,6 +89,9 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
 
 // Mixed-precision thin-disk render: FP32 speculation, FP64 re-trace, resolve.
 size_t mixed_scratch_bytes(const DevTile& tile, int g2);
+// Room for ordering the re-trace list inside a mixed scratch of n_samples
+// samples (order_sample_list's scratch).
+void* mixed_order_scratch(void* scratch, size_t n_samples);
 // phase_events: NULL, or kMixedPhases + 1 events recorded on the stream around
 // the phases (speculate, stars, re-trace, resolve).
 constexpr int kMixedPhases = 4;

@@ -757,6 +757,10 @@ cudaError_t launch_volume_rgb_mixed(const DevScene& S, const DevTile& tile, cons
     e = launch_mixed_stars(S, tile, mb, stream);
     if (e != cudaSuccess) return e;
     mark(2);
+    // the re-trace takes its samples in the FP64 form's order (the longest rays
+    // would otherwise start last)
+    e = order_sample_list(mb.retrace_list, mb.retrace_count, n, mixed_order_scratch(scratch, n), stream);
+    if (e != cudaSuccess) return e;
     e = launch_volume_rgb_retrace(S, tile, mb, res.stats, res.cancel, stream);
     if (e != cudaSuccess) return e;
     mark(3);
