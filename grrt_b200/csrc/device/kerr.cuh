@@ -156,8 +156,9 @@ GRRT_HD Vec5<T> kerr_rhs_body(T M, T a, T pt, T pph, const Vec5<T>& y) {
 }
 
 #ifdef GRRT_RHS_CALL_F64
+// The state is passed by value, so the call passes it in registers.
 static __host__ __device__ __noinline__ Vec5<double> kerr_rhs_f64_call(double M, double a, double pt, double pph,
-                                                                       const Vec5<double>& y) {
+                                                                       Vec5<double> y) {
     return kerr_rhs_body<double>(M, a, pt, pph, y);
 }
 #endif
