@@ -150,6 +150,11 @@ def measured_peaks(torch) -> dict:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         peaks.update(json.load(open(path)))
+        peaks["source"] = "MEASURED_PEAKS.json"
+    else:
+        # an earlier measurement on this pool's B200s (copy bandwidth, cuBLAS
+        # bf16 burst), used when the measured file is absent
+        peaks.update({"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"})
     # FP64 roofline denominator: cuBLAS DGEMM measured here (the same method
     # the driver uses for its bf16 figure), best of 5.
     n = 8192
@@ -595,7 +600,9 @@ def run_surrogate(args, torch, G, stream, flush, peaks):
                          "peak": peak, "unit": "TFLOP/s", "frac": (mlp_tflops / peak) if peak else None,
                          "launch_ms": ms_mlp, "flops_per_launch": F_MLP * rays,
                          "flop_count": f"{F_MLP} per sample (4x256 + 3x256x256 + 256x9 multiply-adds, x2) x {rays}",
-                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)"},
+                         "peak_source": (f"{peaks.get('source')} bf16_tflops (cuBLAS bf16 burst)"
+                                         + ("" if peaks.get("source") == "MEASURED_PEAKS.json" else
+                                            ", of fallback: MEASURED_PEAKS.json absent"))},
         "gpu_launches_per_step": 6,
     }
 
