@@ -627,7 +627,8 @@ def main():
         res["clocks"] = clocks.stop()
         res.update(n_gpus=1, steps=args.steps, warmup=args.warmup, unit="pixel*frequency/s",
                    higher_is_better=True, data="synthetic", dtype="f32+f64",
-                   gpu_launches=args.steps * 3)
+                   # mixed form per frame: speculation, the list ordering's four kernels, re-trace, resolve
+                   gpu_launches=args.steps * 7)
         print(json.dumps(res), flush=True)
         return
     if (args.width, args.height) != (W, H):
