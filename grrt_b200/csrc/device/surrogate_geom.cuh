@@ -136,6 +136,8 @@ GRRT_HD double camera_ray_min_radius(double M, double a, double r_h, double r_ca
 // but the scan stops at r_gate and the bracket that holds r_gate is settled by
 // the sign of R at r_gate (the turning point lies above r_gate exactly when
 // r_gate is in the forbidden region) instead of by bisection.
+// Only signs of R are taken (R and R / (E^2 r^4) have the same sign), so no
+// division is made.
 GRRT_HD bool camera_ray_clears(double M, double a, double r_h, double r_cam, double theta_cam, const double p[4],
                                double r_gate) {
     if (p[1] >= 0.0) return r_cam > r_gate;
@@ -148,10 +150,10 @@ GRRT_HD bool camera_ray_clears(double M, double a, double r_h, double r_cam, dou
         const double r = (i == kN - 1) ? lo : r_prev / q;
         if (r <= r_gate) {
             // R >= 0 at r: any turning point lies below r <= r_gate
-            if (!(scaled_potential(M, a, k, r) < 0.0)) return false;
-            return scaled_potential(M, a, k, r_gate) < 0.0;
+            if (!(radial_potential(M, a, k, r) < 0.0)) return false;
+            return radial_potential(M, a, k, r_gate) < 0.0;
         }
-        if (scaled_potential(M, a, k, r) < 0.0) return true;  // turning point in (r, r_prev), above r_gate
+        if (radial_potential(M, a, k, r) < 0.0) return true;  // turning point in (r, r_prev), above r_gate
         r_prev = r;
     }
     return false;
