@@ -5,7 +5,7 @@
  * spin, inclination) to the quantities a thin-disk pixel's colour is made of;
  * it is trained on the GPU on geodesics the plain FP64 integrator traces, by
  * the library's own BF16 tensor-core (tcgen05) kernels with FP32 accumulation.
- * The plain integrator stays the fallback and the judge: samples the network
+ * The plain integrator stays the fallback and the arbiter: samples the network
  * cannot decide to its calibrated accuracy are re-traced exactly.
  */
 #ifndef GRRT_SURROGATE_H
