@@ -50,6 +50,9 @@ GRRTContext::~GRRTContext() {
         cudaFree(d_spec_scratch);
         cudaFree(d_mixed_scratch);
         if (h_cancel) cudaFreeHost(h_cancel);
+        if (h_stage) cudaFreeHost(h_stage);
+        for (cudaEvent_t& e : ev_copy)
+            if (e) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (cudaEvent_t& e : ev_phase)
@@ -405,6 +408,55 @@ int GRRTContext::wait_with_progress(cudaStream_t s, unsigned total, grrt_progres
     return 0;
 }
 
+// Device-to-host copy of a finished result into caller memory (pageable, as a
+// caller's framebuffer usually is): through a pinned staging buffer in
+// kCopyChunks chunks, each chunk's copy into the caller's buffer spread over
+// the host threads while the next chunks cross the bus. Falls back to one
+// plain copy for small results or when no pinned memory can be had.
+int GRRTContext::copy_to_host(void* host, const void* d, size_t bytes, cudaStream_t s) {
+    constexpr size_t kMin = size_t(4) << 20;
+    if (bytes >= kMin && bytes > h_stage_bytes) {
+        if (h_stage) cudaFreeHost(h_stage);
+        h_stage = nullptr;
+        h_stage_bytes = 0;
+        if (cudaMallocHost(&h_stage, bytes) == cudaSuccess) {
+            h_stage_bytes = bytes;
+        } else {
+            cudaGetLastError();
+            h_stage = nullptr;
+        }
+    }
+    bool events = h_stage != nullptr;
+    for (cudaEvent_t& e : ev_copy)
+        if (events && !e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) events = false;
+    if (bytes < kMin || !events) return fail_cuda(cudaMemcpy(host, d, bytes, cudaMemcpyDeviceToHost), "copy result") ? -1 : 0;
+    const size_t chunk = (bytes + kCopyChunks - 1) / kCopyChunks;
+    for (int k = 0; k < kCopyChunks; ++k) {
+        const size_t off = chunk * k, len = std::min(chunk, bytes - std::min(bytes, off));
+        if (len == 0) break;
+        if (fail_cuda(cudaMemcpyAsync(static_cast<char*>(h_stage) + off, static_cast<const char*>(d) + off, len,
+                                      cudaMemcpyDeviceToHost, s),
+                      "copy result") ||
+            fail_cuda(cudaEventRecord(ev_copy[k], s), "copy result"))
+            return -1;
+    }
+    for (int k = 0; k < kCopyChunks; ++k) {
+        const size_t off = chunk * k, len = std::min(chunk, bytes - std::min(bytes, off));
+        if (len == 0) break;
+        if (fail_cuda(cudaEventSynchronize(ev_copy[k]), "copy result")) return -1;
+        const char* src = static_cast<const char*>(h_stage) + off;
+        char* dst = static_cast<char*>(host) + off;
+        constexpr size_t kPiece = size_t(256) << 10;
+        const long long pieces = static_cast<long long>((len + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < pieces; ++i) {
+            const size_t o = static_cast<size_t>(i) * kPiece;
+            std::memcpy(dst + o, src + o, std::min(kPiece, len - o));
+        }
+    }
+    return 0;
+}
+
 int GRRTContext::render_rgb_to_host(const DevTile& tile, float* host, grrt_progress_fn cb, void* user) {
     if (!ensure_device()) return -1;
     progress = 0.0f;
@@ -416,8 +468,7 @@ int GRRTContext::render_rgb_to_host(const DevTile& tile, float* host, grrt_progr
     }
     if (render_rgb_device(tile, d, nullptr, nullptr, stream, true) != 0) return -1;
     if (wait_with_progress(stream, static_cast<unsigned>(tile.w) * tile.h, cb, user) != 0) return -1;
-    if (fail_cuda(cudaMemcpy(host, d, bytes, cudaMemcpyDeviceToHost), "copy result")) return -1;
-    return 0;
+    return copy_to_host(host, d, bytes, stream);
 }
 
 int GRRTContext::render_spectral_device(int width, int height, double* d_spec, unsigned* d_fate, cudaStream_t s,

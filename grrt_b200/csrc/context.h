@@ -13,6 +13,9 @@
 #include "device/scene.h"
 #include "host/tables.h"
 
+// Chunks of the pipelined device-to-host copy (copy_to_host).
+constexpr int kCopyChunks = 4;
+
 struct GRRTContext {
     GRRTParams params{};
 
@@ -62,6 +65,10 @@ struct GRRTContext {
     // cached device outputs for the host-buffer entry points
     void* d_out = nullptr;
     size_t d_out_bytes = 0;
+    // pinned staging of the host-buffer entry points' device-to-host copy
+    void* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    cudaEvent_t ev_copy[kCopyChunks] = {};
     double* d_freqs = nullptr;
     size_t d_freqs_n = 0;
     double* d_spec_scratch = nullptr;
@@ -96,5 +103,6 @@ struct GRRTContext {
     // helpers
     bool fail_cuda(cudaError_t e, const char* what);
     void* scratch_output(size_t bytes);
+    int copy_to_host(void* host, const void* d, size_t bytes, cudaStream_t s);
     int wait_with_progress(cudaStream_t s, unsigned total_pixels, grrt_progress_fn cb, void* user);
 };
