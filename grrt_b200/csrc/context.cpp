@@ -563,8 +563,7 @@ int GRRTContext::render_spectral_to_host(int width, int height, double* host, gr
     }
     if (render_spectral_device(width, height, d, nullptr, stream, true) != 0) return -1;
     if (wait_with_progress(stream, static_cast<unsigned>(width) * height, cb, user) != 0) return -1;
-    if (fail_cuda(cudaMemcpy(host, d, bytes, cudaMemcpyDeviceToHost), "copy result")) return -1;
-    return 0;
+    return copy_to_host(host, d, bytes, stream);
 }
 
 int GRRTContext::render_spectral_to_fits(const char* path, int width, int height, grrt_progress_fn cb, void* user) {
