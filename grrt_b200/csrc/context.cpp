@@ -356,6 +356,9 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
         }
     }
     n_phases = 0;
+    progress_total = (mixed_thin || mixed_vol) ? static_cast<unsigned>(tile.w) * tile.h * (S.grid * S.grid)
+                                               : static_cast<unsigned>(tile.w) * tile.h;
+    progress_header = (mixed_thin || mixed_vol) ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
     cudaEventRecord(ev0, s);
     cudaError_t e;
     if (mixed_vol)
@@ -374,19 +377,36 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     return 0;
 }
 
-int GRRTContext::wait_with_progress(cudaStream_t s, unsigned total, grrt_progress_fn cb, void* user) {
+int GRRTContext::wait_with_progress(cudaStream_t s, grrt_progress_fn cb, void* user) {
     if (cb) {
-        // Poll the work counter through a second stream while the kernel runs.
+        // Poll the launch's work counters through a second stream while the
+        // kernels run. Single-pass forms count pixels; the mixed forms count
+        // samples in their speculation (the first half of the report) and
+        // re-trace list entries against the list's length (the second half).
         cudaStream_t poll = nullptr;
         unsigned* h_q = nullptr;
         if (cudaStreamCreateWithFlags(&poll, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaMallocHost(&h_q, sizeof(unsigned)) == cudaSuccess) {
+            cudaMallocHost(&h_q, 3 * sizeof(unsigned)) == cudaSuccess) {
             float last = -1.0f;
             while (cudaStreamQuery(s) == cudaErrorNotReady) {
                 std::this_thread::sleep_for(std::chrono::milliseconds(5));
-                if (cudaMemcpyAsync(h_q, d_queue, sizeof(unsigned), cudaMemcpyDeviceToHost, poll) != cudaSuccess) break;
+                h_q[0] = h_q[1] = h_q[2] = 0;
+                if (cudaMemcpyAsync(h_q, d_queue, sizeof(unsigned), cudaMemcpyDeviceToHost, poll) != cudaSuccess)
+                    break;
+                if (progress_header &&
+                    (cudaMemcpyAsync(h_q + 1, progress_header + 256, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                     poll) != cudaSuccess ||
+                     cudaMemcpyAsync(h_q + 2, progress_header + 512, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                     poll) != cudaSuccess))
+                    break;
                 cudaStreamSynchronize(poll);
-                const float f = total ? std::min(1.0f, static_cast<float>(*h_q) / static_cast<float>(total)) : 1.0f;
+                float f = progress_total ? std::min(1.0f, static_cast<float>(h_q[0]) / progress_total) : 1.0f;
+                if (progress_header) {
+                    const float f2 = (f >= 1.0f && h_q[2] > 0)
+                                         ? std::min(1.0f, static_cast<float>(h_q[1]) / static_cast<float>(h_q[2]))
+                                         : 0.0f;
+                    f = 0.5f * f + 0.5f * f2;
+                }
                 if (f > last && f < 1.0f) {
                     progress = f;
                     cb(f, user);
@@ -408,14 +428,11 @@ int GRRTContext::wait_with_progress(cudaStream_t s, unsigned total, grrt_progres
     return 0;
 }
 
-// Device-to-host copy of a finished result into caller memory (pageable, as a
-// caller's framebuffer usually is): through a pinned staging buffer in
-// kCopyChunks chunks, each chunk's copy into the caller's buffer spread over
-// the host threads while the next chunks cross the bus. Falls back to one
-// plain copy for small results or when no pinned memory can be had.
-int GRRTContext::copy_to_host(void* host, const void* d, size_t bytes, cudaStream_t s) {
-    constexpr size_t kMin = size_t(4) << 20;
-    if (bytes >= kMin && bytes > h_stage_bytes) {
+// Pinned host staging of at least `bytes`, kept across calls, and the
+// chunk events of the pipelined copies. False when pinned memory cannot be
+// had (the callers then copy without staging).
+bool GRRTContext::stage_pinned(size_t bytes) {
+    if (bytes > h_stage_bytes) {
         if (h_stage) cudaFreeHost(h_stage);
         h_stage = nullptr;
         h_stage_bytes = 0;
@@ -424,12 +441,27 @@ int GRRTContext::copy_to_host(void* host, const void* d, size_t bytes, cudaStrea
         } else {
             cudaGetLastError();
             h_stage = nullptr;
+            return false;
         }
     }
-    bool events = h_stage != nullptr;
     for (cudaEvent_t& e : ev_copy)
-        if (events && !e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) events = false;
-    if (bytes < kMin || !events) return fail_cuda(cudaMemcpy(host, d, bytes, cudaMemcpyDeviceToHost), "copy result") ? -1 : 0;
+        if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            e = nullptr;
+            return false;
+        }
+    return h_stage != nullptr;
+}
+
+// Device-to-host copy of a finished result into caller memory (pageable, as a
+// caller's framebuffer usually is): through a pinned staging buffer in
+// kCopyChunks chunks, each chunk's copy into the caller's buffer spread over
+// the host threads while the next chunks cross the bus. Falls back to one
+// plain copy for small results or when no pinned memory can be had.
+int GRRTContext::copy_to_host(void* host, const void* d, size_t bytes, cudaStream_t s) {
+    constexpr size_t kMin = size_t(4) << 20;
+    const bool events = bytes >= kMin && stage_pinned(bytes);
+    if (!events) return fail_cuda(cudaMemcpy(host, d, bytes, cudaMemcpyDeviceToHost), "copy result") ? -1 : 0;
     const size_t chunk = (bytes + kCopyChunks - 1) / kCopyChunks;
     for (int k = 0; k < kCopyChunks; ++k) {
         const size_t off = chunk * k, len = std::min(chunk, bytes - std::min(bytes, off));
@@ -467,7 +499,7 @@ int GRRTContext::render_rgb_to_host(const DevTile& tile, float* host, grrt_progr
         return -1;
     }
     if (render_rgb_device(tile, d, nullptr, nullptr, stream, true) != 0) return -1;
-    if (wait_with_progress(stream, static_cast<unsigned>(tile.w) * tile.h, cb, user) != 0) return -1;
+    if (wait_with_progress(stream, cb, user) != 0) return -1;
     return copy_to_host(host, d, bytes, stream);
 }
 
@@ -483,6 +515,8 @@ int GRRTContext::render_spectral_device(int width, int height, double* d_spec, u
         // No volumetric disk: the reference returns all-zero spectra
         // (src/geodesic_tracer.cpp:503-505).
         n_phases = 0;
+        progress_total = 0;
+        progress_header = nullptr;
         cudaEventRecord(ev0, s);
         cudaError_t e = cudaMemsetAsync(d_spec, 0, n * sizeof(double), s);
         if (d_fate && e == cudaSuccess) {
@@ -542,6 +576,9 @@ int GRRTContext::render_spectral_device(int width, int height, double* d_spec, u
         }
     }
     n_phases = 0;
+    progress_total = mixed ? static_cast<unsigned>(width) * height * (S.grid * S.grid)
+                           : static_cast<unsigned>(width) * height;
+    progress_header = mixed ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
     cudaEventRecord(ev0, s);
     const cudaError_t e =
         mixed ? launch_volume_spectral_mixed(S, tile, d_freqs, nb, out, res, d_mixed_scratch, d_mixed_scratch_bytes,
@@ -562,7 +599,7 @@ int GRRTContext::render_spectral_to_host(int width, int height, double* host, gr
         return -1;
     }
     if (render_spectral_device(width, height, d, nullptr, stream, true) != 0) return -1;
-    if (wait_with_progress(stream, static_cast<unsigned>(width) * height, cb, user) != 0) return -1;
+    if (wait_with_progress(stream, cb, user) != 0) return -1;
     return copy_to_host(host, d, bytes, stream);
 }
 
@@ -578,28 +615,55 @@ int GRRTContext::render_spectral_to_fits(const char* path, int width, int height
     meta.samples_per_pixel = params.samples_per_pixel > 0 ? params.samples_per_pixel : 1;
     const int nb = static_cast<int>(freq_bins.size());
     const size_t cube = static_cast<size_t>(width) * height * nb;
-    // The cube lives on the device; one big-endian plane at a time crosses to
-    // the host, so host memory stays at two planes whatever the cube size.
-    const size_t plane = static_cast<size_t>(width) * height;
-    auto* d = static_cast<unsigned char*>(scratch_output(sizeof(double) * (cube + plane)));
+    const size_t plane_bytes = sizeof(double) * static_cast<size_t>(width) * height;
+    // The rendered cube and its big-endian FITS image side by side on the device.
+    auto* d = static_cast<unsigned char*>(scratch_output(2 * sizeof(double) * cube));
     if (!d) {
         error = "cudaMalloc(cube) failed";
         return -1;
     }
     double* d_cube = reinterpret_cast<double*>(d);
-    unsigned char* d_plane = d + sizeof(double) * cube;
+    unsigned char* d_be = d + sizeof(double) * cube;
     try {
         FitsCubeWriter writer(path, width, height, nb, freq_bins, meta);
         if (render_spectral_device(width, height, d_cube, nullptr, stream, true) != 0) return -1;
-        if (wait_with_progress(stream, static_cast<unsigned>(width) * height, cb, user) != 0) return -1;
-        std::vector<unsigned char> host(plane * sizeof(double));
-        for (int k = 0; k < nb; ++k) {
-            if (fail_cuda(pack_fits_plane(d_cube, width, height, nb, k, d_plane, stream), "pack plane")) return -1;
-            if (fail_cuda(cudaMemcpyAsync(host.data(), d_plane, host.size(), cudaMemcpyDeviceToHost, stream),
-                          "copy plane"))
-                return -1;
-            if (fail_cuda(cudaStreamSynchronize(stream), "copy plane")) return -1;
-            writer.write_plane(k, host.data());
+        if (wait_with_progress(stream, cb, user) != 0) return -1;
+        // The FITS data section is the planes back to back, so the packed cube
+        // goes to the file as it is. Planes are packed and copied in groups on
+        // the render stream; each group is written to the file while the next
+        // groups are packed and cross the bus.
+        const int groups = std::min(kCopyChunks, nb);
+        const int per = (nb + groups - 1) / groups;
+        if (stage_pinned(sizeof(double) * cube)) {
+            auto* h = static_cast<unsigned char*>(h_stage);
+            for (int g = 0; g < groups; ++g) {
+                const int k0 = g * per, k1 = std::min(nb, k0 + per);
+                if (k0 >= k1) break;
+                const size_t off = plane_bytes * static_cast<size_t>(k0);
+                if (fail_cuda(pack_fits_planes(d_cube, width, height, nb, k0, k1, d_be + off, stream), "pack planes") ||
+                    fail_cuda(cudaMemcpyAsync(h + off, d_be + off, plane_bytes * static_cast<size_t>(k1 - k0),
+                                              cudaMemcpyDeviceToHost, stream),
+                              "copy planes") ||
+                    fail_cuda(cudaEventRecord(ev_copy[g], stream), "copy planes"))
+                    return -1;
+            }
+            for (int g = 0; g < groups; ++g) {
+                const int k0 = g * per, k1 = std::min(nb, k0 + per);
+                if (k0 >= k1) break;
+                if (fail_cuda(cudaEventSynchronize(ev_copy[g]), "copy planes")) return -1;
+                writer.write_planes(k0, k1, h + plane_bytes * static_cast<size_t>(k0));
+            }
+        } else {
+            // no pinned memory: one plane at a time through pageable memory
+            std::vector<unsigned char> host(plane_bytes);
+            for (int k = 0; k < nb; ++k) {
+                if (fail_cuda(pack_fits_planes(d_cube, width, height, nb, k, k + 1, d_be, stream), "pack plane") ||
+                    fail_cuda(cudaMemcpyAsync(host.data(), d_be, plane_bytes, cudaMemcpyDeviceToHost, stream),
+                              "copy plane") ||
+                    fail_cuda(cudaStreamSynchronize(stream), "copy plane"))
+                    return -1;
+                writer.write_planes(k, k + 1, host.data());
+            }
         }
         writer.finalize();
     } catch (const std::exception& e) {

@@ -44,6 +44,11 @@ struct GRRTContext {
 
     std::string error;
     float progress = 0.0f;
+    // work counters of the last launch that progress reports read: the work
+    // counter (d_queue) runs to progress_total; the mixed forms also have a
+    // scratch header with the re-trace counter (+256) and list length (+512)
+    unsigned progress_total = 0;
+    const unsigned char* progress_header = nullptr;
 
     // Device state (created at the first render).
     int device = -1;
@@ -103,6 +108,7 @@ struct GRRTContext {
     // helpers
     bool fail_cuda(cudaError_t e, const char* what);
     void* scratch_output(size_t bytes);
+    bool stage_pinned(size_t bytes);
     int copy_to_host(void* host, const void* d, size_t bytes, cudaStream_t s);
-    int wait_with_progress(cudaStream_t s, unsigned total_pixels, grrt_progress_fn cb, void* user);
+    int wait_with_progress(cudaStream_t s, grrt_progress_fn cb, void* user);
 };

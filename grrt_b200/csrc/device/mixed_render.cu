@@ -28,6 +28,7 @@
 
 #include <cstdint>
 
+#include "launch_cache.h"
 #include "integrate.cuh"
 #include "mixed_spec.cuh"
 #include "render_launch.h"
@@ -151,6 +152,15 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 // pass gains more from the fifth block's warps than it loses to the few
 // spilled registers (four blocks: 8.8 ms, five: 8.2 ms on the 1024x1024 4-spp
 // frame on B200; six, with more spills, no better).
+// True on every lane of the warp once the host has raised the cancel flag
+// (a host-mapped word; lane 0 reads it). Callers poll every 1024 loop
+// iterations, as the FP64 kernels do.
+__device__ __forceinline__ bool cancel_requested(const volatile int* cancel) {
+    int c = 0;
+    if ((threadIdx.x & 31u) == 0) c = *cancel;
+    return __shfl_sync(kMask, c, 0) != 0;
+}
+
 template <bool kBatch>
 __global__ void __launch_bounds__(kMixThreads, 5)
 mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
@@ -170,6 +180,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
     bool settled = false;  // black sky, never reaches the disk: final without a trace
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0;
+    unsigned iter = 0;
     mixed::Tracker trk;
     while (true) {
         const bool want = !live && !exhausted;
@@ -209,6 +220,7 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
             }
         }
         if (!__any_sync(kMask, live)) break;
+        if (mb.cancel && ((++iter & 1023u) == 0) && cancel_requested(mb.cancel)) break;
         int term = -1;
         bool retrace = false;
         Vec5<float> k7;
@@ -323,6 +335,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
     bool k1_ok = false;
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0, ncross = 0;
+    unsigned iter = 0;
     double c0 = 0, c1 = 0, c2 = 0;
     while (true) {
         const bool want = !live && !exhausted;
@@ -343,6 +356,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
             }
         }
         if (!__any_sync(kMask, live)) break;
+        if (mb.cancel && ((++iter & 1023u) == 0) && cancel_requested(mb.cancel)) break;
         int term = -1;
         if (live && retry == 0) term = start_test(S, step, y.r);
         if (live && term < 0) {
@@ -503,10 +517,8 @@ struct MixLaunchShape {
     int per_spec_b = 1, per_retrace_b = 1;  // the batch instantiations
 };
 const MixLaunchShape& mix_shape() {
-    static MixLaunchShape sh;
-    if (sh.sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
+    return per_device_shape<MixLaunchShape>([](int dev) {
+        MixLaunchShape sh;
         cudaDeviceGetAttribute(&sh.sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, mixed_speculate_kernel<false>, kMixThreads, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, mixed_retrace_kernel<false>, kMixThreads, 0);
@@ -516,8 +528,8 @@ const MixLaunchShape& mix_shape() {
         if (sh.per_retrace < 1) sh.per_retrace = 1;
         if (sh.per_spec_b < 1) sh.per_spec_b = 1;
         if (sh.per_retrace_b < 1) sh.per_retrace_b = 1;
-    }
-    return sh;
+        return sh;
+    });
 }
 }  // namespace
 
@@ -596,6 +608,7 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     DevMixedBuffers mb = mixed_buffers(scratch, n, res.queue);
     mb.margin = margin;
     mb.r_near = r_near;
+    mb.cancel = res.cancel;
     cudaError_t e = cudaMemsetAsync(scratch, 0, 1024, stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);

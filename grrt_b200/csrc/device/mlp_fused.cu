@@ -34,6 +34,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "launch_cache.h"
 #include "mlp_fused.h"
 #include "sm100.cuh"
 #include "surrogate.h"
@@ -354,17 +355,20 @@ cudaError_t launch_mlp_fused(const float* X, long long n, const float* params, _
     for (int l = 0; l < 3; ++l)
         if (!weight_map(&maps.w[l], wb[l], kHidden)) return cudaErrorInvalidValue;
     if (!weight_map(&maps.w[3], w5b, kOutPad)) return cudaErrorInvalidValue;
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    static int sms = 0;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(mlp_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(mlp_fused_smem_bytes()));
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    struct Shape {
+        cudaError_t attr = cudaSuccess;
+        int sms = 0;
+    };
+    // the shared-memory attribute is set once per device, with that device current
+    const Shape& sh = per_device_shape<Shape>([](int dev) {
+        Shape v;
+        v.attr = cudaFuncSetAttribute(mlp_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(mlp_fused_smem_bytes()));
+        cudaDeviceGetAttribute(&v.sms, cudaDevAttrMultiProcessorCount, dev);
+        return v;
     });
-    if (attr != cudaSuccess) return attr;
+    if (sh.attr != cudaSuccess) return sh.attr;
+    const int sms = sh.sms;
     const long long tiles = (n + kRows - 1) / kRows;
     const int grid = static_cast<int>(tiles < sms ? tiles : sms);
     mlp_fused_kernel<<<grid, kThreads, mlp_fused_smem_bytes(), s>>>(maps, X, n, d_n, params, out, d_err);

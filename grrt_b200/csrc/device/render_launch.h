@@ -36,6 +36,7 @@ struct DevMixedBuffers {
     uint32_t* sample_fate = nullptr;    // per sample
     double margin = 0.05;               // disk-radius margin of the re-trace test
     double r_near = 0.0;                // escapes after coming inside r_near are re-traced
+    const volatile int* cancel = nullptr;  // host-mapped cancel flag (single renders), may be null
 };
 
 // Scratch a launch uses beside its inputs and outputs.

@@ -20,6 +20,7 @@
 
 #include <cstdint>
 
+#include "launch_cache.h"
 #include "integrate.cuh"
 #include "render_launch.h"
 #include "shading.cuh"
@@ -297,15 +298,17 @@ thin_batch_kernel(const __grid_constant__ DevBatch B, float4* __restrict__ out_r
 
 cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                         const LaunchResources& res, cudaStream_t stream) {
-    static int blocks_per_sm = 0;
-    static int num_sms = 0;
-    if (blocks_per_sm == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, thin_render_kernel, kThreads, 0);
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-    }
+    struct Shape {
+        int sms = 0, per = 1;
+    };
+    const Shape& sh = per_device_shape<Shape>([](int dev) {
+        Shape v;
+        cudaDeviceGetAttribute(&v.sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.per, thin_render_kernel, kThreads, 0);
+        if (v.per < 1) v.per = 1;
+        return v;
+    });
+    const int num_sms = sh.sms, blocks_per_sm = sh.per;
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
     if (total == 0) return cudaSuccess;
     int blocks = num_sms * blocks_per_sm;

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "launch_cache.h"
 #include "sm100.cuh"
 #include "umma_gemm.h"
 
@@ -237,13 +238,17 @@ cudaError_t umma_gemm_bf16(const __nv_bfloat16* A, int lda, const __nv_bfloat16*
     const int per = (kbt + splits - 1) / splits;
     splits = (kbt + per - 1) / per;  // every split gets at least one K-block
     const size_t smem = umma_gemm_smem_bytes(N);
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(umma_gemm_smem_bytes(256)));
+    // the shared-memory attribute is set once per device, with that device current
+    struct Attr {
+        cudaError_t err = cudaSuccess;
+    };
+    const Attr& attr = per_device_shape<Attr>([](int) {
+        Attr a;
+        a.err = cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(umma_gemm_smem_bytes(256)));
+        return a;
     });
-    if (attr_err != cudaSuccess) return attr_err;
+    if (attr.err != cudaSuccess) return attr.err;
     dim3 grid((M + kBM - 1) / kBM, splits);
     umma_gemm_kernel<<<grid, kThreads, smem, stream>>>(ta, tb, ep, M, N, per, kbt, d_err);
     return cudaGetLastError();

@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "launch_cache.h"
 #include "integrate.cuh"
 #include "render_launch.h"
 #include "shading.cuh"
@@ -240,19 +241,21 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
 }
 
 namespace {
+struct VolRgbShape {
+    int sms = 0, per[2] = {1, 1};
+};
 int vol_rgb_blocks_per_sm(bool list, int& sms) {
-    static int per[2] = {0, 0}, num_sms = 0;
-    if (num_sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], vol_render_kernel<false>, kVolThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], vol_render_kernel<true>, kVolThreads, 0);
-        for (int& p : per)
+    const VolRgbShape& sh = per_device_shape<VolRgbShape>([](int dev) {
+        VolRgbShape v;
+        cudaDeviceGetAttribute(&v.sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.per[0], vol_render_kernel<false>, kVolThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.per[1], vol_render_kernel<true>, kVolThreads, 0);
+        for (int& p : v.per)
             if (p < 1) p = 1;
-    }
-    sms = num_sms;
-    return per[list ? 1 : 0];
+        return v;
+    });
+    sms = sh.sms;
+    return sh.per[list ? 1 : 0];
 }
 }  // namespace
 
@@ -287,8 +290,7 @@ cudaError_t launch_volume_rgb_retrace(const DevScene& S, const DevTile& tile, co
 //
 // For callers that must not allocate device memory while they render: a host
 // application that hands the renderer a fixed memory budget and forbids
-// driver allocations during a frame, a pipeline recorded into a CUDA graph
-// (cudaMalloc cannot be captured), or a process running near the device
+// driver allocations during a frame, or a process running near the device
 // memory limit where an allocation could fail mid-frame. The per-launch
 // scratch (work counter, counters, and the per-lane J, T, tau and pixel-sum
 // transfer state) lives in the file-scope array below instead of cudaMalloc'd

@@ -35,6 +35,7 @@
 
 #include <cstdint>
 
+#include "launch_cache.h"
 #include "integrate.cuh"
 #include "mixed_spec.cuh"
 #include "render_launch.h"
@@ -610,10 +611,8 @@ struct SpecShape {
     int sms = 0, per_fp64 = 1, per_list = 1, per_spec = 1, per_spec_rgb = 1;
 };
 const SpecShape& spec_shape() {
-    static SpecShape sh;
-    if (sh.sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
+    return per_device_shape<SpecShape>([](int dev) {
+        SpecShape sh;
         cudaDeviceGetAttribute(&sh.sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_fp64, vol_spectral_kernel<false>, kSpecThreads, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_list, vol_spectral_kernel<true>, kSpecThreads, 0);
@@ -623,8 +622,8 @@ const SpecShape& spec_shape() {
         if (sh.per_fp64 < 1) sh.per_fp64 = 1;
         if (sh.per_list < 1) sh.per_list = 1;
         if (sh.per_spec < 1) sh.per_spec = 1;
-    }
-    return sh;
+        return sh;
+    });
 }
 }  // namespace
 

@@ -138,11 +138,11 @@ FitsCubeWriter::~FitsCubeWriter() {
     if (f_) std::fclose(f_);
 }
 
-void FitsCubeWriter::write_plane(int k, const void* plane_be) {
-    if (k != next_plane_) throw std::runtime_error("grrt: FITS planes must be written in order");
-    const size_t n = static_cast<size_t>(width_) * height_ * 8;
-    if (std::fwrite(plane_be, 1, n, f_) != n) throw std::runtime_error("grrt: write error on '" + path_ + "'");
-    ++next_plane_;
+void FitsCubeWriter::write_planes(int k0, int k1, const void* planes_be) {
+    if (k0 != next_plane_ || k1 < k0 || k1 > bins_) throw std::runtime_error("grrt: FITS planes must be written in order");
+    const size_t n = static_cast<size_t>(width_) * height_ * 8 * static_cast<size_t>(k1 - k0);
+    if (std::fwrite(planes_be, 1, n, f_) != n) throw std::runtime_error("grrt: write error on '" + path_ + "'");
+    next_plane_ = k1;
 }
 
 void FitsCubeWriter::finalize() {

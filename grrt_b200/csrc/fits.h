@@ -21,7 +21,9 @@ struct FitsMetadata {
 std::vector<std::string> fits_header_cards(int width, int height, int num_bins,
                                            const std::vector<double>& freqs, const FitsMetadata& meta);
 
-// Writes the header on construction, then whole frequency planes in order.
+// Writes the header on construction, then whole frequency planes in order
+// (the data section is contiguous: plane k starts k * width * height * 8
+// bytes after the header).
 class FitsCubeWriter {
 public:
     FitsCubeWriter(const std::string& path, int width, int height, int num_bins,
@@ -29,8 +31,9 @@ public:
     ~FitsCubeWriter();
     FitsCubeWriter(const FitsCubeWriter&) = delete;
     FitsCubeWriter& operator=(const FitsCubeWriter&) = delete;
-    // plane_be: width*height big-endian doubles of plane k, FITS row order.
-    void write_plane(int k, const void* plane_be);
+    // planes_be: planes [k0, k1), each width*height big-endian doubles in
+    // FITS row order, back to back; k0 must be the next unwritten plane.
+    void write_planes(int k0, int k1, const void* planes_be);
     void finalize();
 
 private:
@@ -40,9 +43,10 @@ private:
     int next_plane_ = 0;
 };
 
-// Device: converts plane k of a [pixel][bin] double cube into big-endian
-// doubles in FITS order (row j of the image becomes FITS row height-1-j).
-cudaError_t pack_fits_plane(const double* cube, int width, int height, int num_bins, int k,
-                            unsigned char* out_be, cudaStream_t stream);
+// Device: converts planes [k0, k1) of a [pixel][bin] double cube into
+// big-endian doubles in FITS order (row j of the image becomes FITS row
+// height-1-j), plane after plane into out_be.
+cudaError_t pack_fits_planes(const double* cube, int width, int height, int num_bins, int k0, int k1,
+                             unsigned char* out_be, cudaStream_t stream);
 
 }  // namespace grrt_b200

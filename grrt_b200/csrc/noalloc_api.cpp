@@ -32,14 +32,22 @@ extern "C" GRRT_EXPORT int grrt_render_spectral_device_noalloc(GRRTContext* ctx,
                      "render call on this context (any other grrt_render* entry point) uploads it";
         return -1;
     }
-    if (!ctx->vol) {
-        ctx->error = "grrt_render_spectral_device_noalloc: the context has no volumetric disk";
-        return -1;
-    }
     if (cudaSetDevice(ctx->device) != cudaSuccess) {
         cudaGetLastError();
         ctx->error = "grrt_render_spectral_device_noalloc: cannot select the context's device";
         return -1;
+    }
+    if (!ctx->vol) {
+        // No volumetric disk: all-zero spectra, as grrt_render_spectral_device
+        // and the reference give (src/geodesic_tracer.cpp:503-505).
+        const size_t bytes = sizeof(double) * static_cast<size_t>(width) * height * num_bins;
+        const cudaError_t z = cudaMemsetAsync(d_spec, 0, bytes, static_cast<cudaStream_t>(stream));
+        if (z != cudaSuccess) {
+            ctx->error = std::string("grrt_render_spectral_device_noalloc: ") + cudaGetErrorString(z);
+            cudaGetLastError();
+            return -1;
+        }
+        return 0;
     }
     DevTile tile;
     tile.w = width;

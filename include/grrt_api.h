@@ -151,9 +151,12 @@ GRRT_EXPORT int grrt_render_spectral(GRRTContext* ctx, double* spectral_buffer,
 GRRT_EXPORT int grrt_render_spectral_cb(GRRTContext* ctx, double* spectral_buffer,
                                         int width, int height,
                                         grrt_progress_fn progress, void* user_data);
-/* api.h:47-51 / api.cpp:283-332: streams the cube to a FITS file (BITPIX -64,
- * big-endian, rows flipped) a band of rows at a time; 0 on success, -1 with
- * grrt_error(ctx) set. */
+/* api.h:47-51 / api.cpp:283-332: writes the cube to a FITS file (BITPIX -64,
+ * big-endian, rows flipped; byte-identical to the reference's file). The
+ * whole cube is rendered on the device first; then the GPU packs it into
+ * FITS order in groups of frequency planes, and each group is written to the
+ * file while the next groups cross the bus. Host memory: one pinned copy of
+ * the cube, kept by the context. 0 on success, -1 with grrt_error(ctx) set. */
 GRRT_EXPORT int grrt_render_spectral_to_fits_cb(GRRTContext* ctx,
                                                 const char* output_path,
                                                 int width, int height,

@@ -100,16 +100,16 @@ GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double* d_spec, in
  *
  * For callers that may not allocate device memory while they render: a host
  * application that gives the renderer a fixed memory budget and forbids
- * driver allocations during a frame, work recorded into a CUDA graph
- * (cudaMalloc cannot be captured), or a process near the device memory limit
- * where an allocation could fail mid-frame. Instead of cudaMalloc'd scratch it
+ * driver allocations during a frame, or a process near the device memory
+ * limit where an allocation could fail mid-frame. Instead of cudaMalloc'd scratch it
  * uses a fixed array compiled into the library (about 19.4 MB on every GPU that
  * loads it, held until the process exits). The caller passes the inputs and
  * outputs: d_freqs (num_bins observer-frame frequencies in Hz, device memory)
  * and d_spec (double[width*height*num_bins], device memory); the scene comes
  * from the context, which must already hold it on the device (any earlier
  * render call on the context uploads it). Same output as
- * grrt_render_spectral_device, enqueued on `stream`.
+ * grrt_render_spectral_device, enqueued on `stream`; a context without a
+ * volumetric disk gets all-zero spectra, as there.
  *
  * Limits: num_bins <= 32, otherwise -1 with grrt_error set. The first call on
  * each device looks up the array's device address; make that first call before

@@ -13,6 +13,12 @@ every double written as float.hex() so the comparison is bit-exact:
     scene,
   * the stratified-jitter hash on a few arguments.
 
+It also writes tests/golden/reference_fits.json: FITS cubes written by the
+reference's own grrt_render_spectral_to_fits_cb (src/api.cpp:283-332, the
+streaming writer of src/fits_writer.cpp:315-395) for three frequency-axis
+kinds (log-uniform, linear-uniform, tabulated), each with its header bytes
+(latin-1 text), file size and data section (big-endian doubles as hex).
+
 Run from the repository root:  python tests/golden/make_golden.py
 """
 from __future__ import annotations
@@ -33,6 +39,61 @@ import grrt_b200 as G  # noqa: E402
 from oracle_bind import RefScene, jittered_samples  # noqa: E402
 
 OUT = os.path.join(HERE, "reference_vectors.json")
+OUT_FITS = os.path.join(HERE, "reference_fits.json")
+
+# (name, scene overrides of the volumetric scene (config 3), frequencies)
+FITS_CASES = [
+    ("log32_16x12", dict(width=16, height=12), ("log", 1e14, 1e18, 32)),
+    ("linear5_13x7_spp4", dict(width=13, height=7, samples_per_pixel=4), ("list", 1e14, 2e14, 3e14, 4e14, 5e14)),
+    ("table3_9x5", dict(width=9, height=5, spin=0.5), ("list", 1e14, 3e15, 2e17)),
+]
+
+
+def fits_case_freqs(spec) -> np.ndarray:
+    if spec[0] == "log":
+        return G.log_bins(spec[1], spec[2], spec[3])
+    return np.array(spec[1:], dtype=np.float64)
+
+
+def fits_vectors() -> None:
+    """FITS files written by the reference's C API (strict build)."""
+    import ctypes as C
+    import tempfile
+    ref_api = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libgrrt_ref_strict.so"))
+    ref_api.grrt_create.restype = C.c_void_p
+    ref_api.grrt_create.argtypes = [C.POINTER(G.GRRTParams)]
+    ref_api.grrt_set_frequency_bins.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+    ref_api.grrt_render_spectral_to_fits_cb.restype = C.c_int
+    ref_api.grrt_render_spectral_to_fits_cb.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p,
+                                                        C.c_void_p]
+    ref_api.grrt_destroy.argtypes = [C.c_void_p]
+    out = {"generator": "tests/golden/make_golden.py", "build": "oracle/_ref/libgrrt_ref_strict.so", "cases": {}}
+    for name, over, fspec in FITS_CASES:
+        vals = G.config_params(3, **over)
+        freqs = fits_case_freqs(fspec)
+        prm = G.make_params(vals, freqs)
+        ctx = ref_api.grrt_create(C.byref(prm))
+        assert ctx, name
+        ref_api.grrt_set_frequency_bins(ctx, freqs.ctypes.data_as(C.POINTER(C.c_double)), len(freqs))
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "ref.fits")
+            rc = ref_api.grrt_render_spectral_to_fits_cb(ctx, path.encode(), vals["width"], vals["height"], None,
+                                                         None)
+            assert rc == 0, name
+            raw = open(path, "rb").read()
+        ref_api.grrt_destroy(ctx)
+        # header: 80-character cards up to END, padded to 2880-byte blocks
+        end = 0
+        while raw[end:end + 3] != b"END":
+            end += 80
+        hdr_len = (end // 2880 + 1) * 2880
+        n = vals["width"] * vals["height"] * len(freqs)
+        data = np.frombuffer(raw[hdr_len:hdr_len + 8 * n], dtype=">f8")
+        out["cases"][name] = {"params": vals, "freqs": hexlist(freqs), "size": len(raw),
+                              "header": raw[:hdr_len].decode("latin-1"), "data": hexlist(data)}
+    with open(OUT_FITS, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", OUT_FITS, os.path.getsize(OUT_FITS), "bytes")
 
 
 def digest(a: np.ndarray) -> str:
@@ -128,6 +189,7 @@ def main() -> None:
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
+    fits_vectors()
 
 
 if __name__ == "__main__":

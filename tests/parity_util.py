@@ -52,6 +52,15 @@ def rel_err(a, b, floor=1e-300):
     return np.abs(a - b) / np.maximum(np.abs(b), floor)
 
 
+def hull_error(got: np.ndarray, lo: np.ndarray, hi: np.ndarray, floor: float = 1e-300) -> np.ndarray:
+    """Per pixel, the largest relative distance (over channels or bins) of
+    `got` outside [lo, hi]: the range spanned by the oracle and its rounding
+    probes. 0 when every channel lies inside it."""
+    scale = np.maximum(np.maximum(np.abs(lo), np.abs(hi)), floor)
+    out = np.maximum(lo - got, got - hi)
+    return np.max(np.maximum(out, 0.0) / scale, axis=1)
+
+
 def pixel_mean(per_sample: np.ndarray, spp: int) -> np.ndarray:
     """The reference's spp mean: accumulate samples in order from 0, then scale."""
     grid = max(1, int(math.sqrt(spp)))
@@ -77,6 +86,7 @@ class OracleRGB:
         self.rgb, self.term, self.ncross, self.fin, self.counters = O.trace_rgb(px, py)
         self.sensitive = np.zeros(len(px), dtype=bool)
         self.fate_sensitive = np.zeros(len(px), dtype=bool)
+        lo, hi = self.rgb.copy(), self.rgb.copy()
         if band:
             F = oracle_bind.Oracle(R, fma=True)
             probes = [F.trace_rgb(px, py)]
@@ -87,7 +97,10 @@ class OracleRGB:
                 self.fate_sensitive |= fs
                 self.sensitive |= fs
                 self.sensitive |= np.any(np.abs(r2 - self.rgb) > tol * np.abs(self.rgb), axis=1)
+                lo, hi = np.minimum(lo, r2), np.maximum(hi, r2)
         self.pixel_rgb = pixel_mean(self.rgb, spp)
+        # per pixel, the range the oracle and its rounding probes span
+        self.pixel_lo, self.pixel_hi = pixel_mean(lo, spp), pixel_mean(hi, spp)
         self.pixel_band = self.sensitive.reshape(-1, self.g2).any(axis=1)
         self.pixel_fate_band = self.fate_sensitive.reshape(-1, self.g2).any(axis=1)
         self.fate = (self.term.astype(np.uint32) | (self.ncross.astype(np.uint32) << 2))
@@ -103,6 +116,7 @@ class OracleSpectral:
         self.spec, self.term, self.counters = O.trace_spectral(freqs, px, py)
         self.sensitive = np.zeros(len(px), dtype=bool)
         self.fate_sensitive = np.zeros(len(px), dtype=bool)
+        lo, hi = self.spec.copy(), self.spec.copy()
         if band:
             F = oracle_bind.Oracle(R, fma=True)
             probes = [F.trace_spectral(freqs, px, py)]
@@ -112,6 +126,8 @@ class OracleSpectral:
                 self.fate_sensitive |= t2 != self.term
                 self.sensitive |= t2 != self.term
                 self.sensitive |= np.any(np.abs(s2 - self.spec) > tol * np.abs(self.spec), axis=1)
+                lo, hi = np.minimum(lo, s2), np.maximum(hi, s2)
         self.pixel_spec = pixel_mean(self.spec, spp)
+        self.pixel_lo, self.pixel_hi = pixel_mean(lo, spp), pixel_mean(hi, spp)
         self.pixel_band = self.sensitive.reshape(-1, self.g2).any(axis=1)
         self.pixel_fate_band = self.fate_sensitive.reshape(-1, self.g2).any(axis=1)
