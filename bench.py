@@ -212,7 +212,13 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP},
+            "data": "synthetic",
+            # the GPU arm's workload keys; the rays of each step are a sample of the frame
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "rays_per_step": RAYS,
+                       "form": "reference FP64 (src/*.cpp)", "l2": "not applicable (host CPU)",
+                       "parallelism": "OpenMP over all host threads (rank 0 only)",
+                       "row_sampling": f"every {stride}th row per step, offset rotating with the step "
+                                       f"({rows} rows = {rows * 1024 * SPP} rays per step)"},
             "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads,
                              "kind": "reference" if kind else "port", "sample": sample},
             "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -404,7 +410,11 @@ def run_volumetric(args, torch, G, stream, flush, p64):
     freqs = G.log_bins(1e14, 1e18, 32)
     vw = vh = args.vol_size
     nb = len(freqs)
+    # context creation (host tables: Saha/opacity grid, disk structure, noise),
+    # timed on the host; the reference's constructor is timed beside it below
+    t_create = time.perf_counter()
     R = G.Renderer(G.config_params(3, width=vw, height=vh), freqs=freqs)
+    create_ms = 1e3 * (time.perf_counter() - t_create)
     spec = torch.empty((vh, vw, nb), dtype=torch.float64, device="cuda")
     fate = torch.empty((vh * vw,), dtype=torch.int32, device="cuda")
     out = {}
@@ -431,6 +441,19 @@ def run_volumetric(args, torch, G, stream, flush, p64):
                      "stats": {k: st[k] for k in ("attempts", "fp64_attempts", "march_steps", "clamp_evals",
                                                   "physics_steps", "bin_updates", "rays", "horizon", "escaped")},
                      "spec": spec.cpu().numpy(), "fate": fate.cpu().numpy()}
+    # the same frame to a FITS cube (grrt_render_spectral_to_fits_cb, mixed
+    # form): host wall clock per call, written to tmpfs so the disk is not timed
+    fits_dir = "/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir()
+    fits_path = os.path.join(fits_dir, f"grrt_bench_{os.getpid()}.fits")
+    R.set_precision(G.FORM_MIXED)
+    R.render_fits(fits_path, vw, vh)  # warm-up: pinned staging and device buffers
+    tf = []
+    for _ in range(max(3, args.steps // 2)):
+        t0 = time.perf_counter()
+        R.render_fits(fits_path, vw, vh)
+        tf.append(1e3 * (time.perf_counter() - t0))
+    fits_bytes = os.path.getsize(fits_path)
+    os.unlink(fits_path)
     f, m = out["fp64"], out["mixed"]
     scale = float(f["spec"].max())
     rel = np.abs(m["spec"] - f["spec"]) / np.maximum(np.abs(f["spec"]), 1e-6 * scale)
@@ -457,13 +480,20 @@ def run_volumetric(args, torch, G, stream, flush, p64):
                              "flop_count": f"{F_ATTEMPT_EXEC}/attempt + {F_EVAL}/ray (first right-hand side), "
                                            f"{F_RK4}/march step, {F_BIN}/bin update (transcendentals and the "
                                            f"right-hand sides after march ends not counted), device counters"},
-           "cube_store": {"bytes": cube, "GB_per_s": cube / (kms * 1e-3) / 1e9}}
+           "cube_store": {"bytes": cube, "GB_per_s": cube / (kms * 1e-3) / 1e9},
+           "create_ms": {"ours": create_ms, "host_threads": os.cpu_count()},
+           "to_fits": {"ms_per_frame": float(np.median(tf)), "device_ms_per_frame": m["ms_per_step"],
+                       "file_bytes": fits_bytes, "target": fits_dir,
+                       "api": "grrt_render_spectral_to_fits_cb (mixed form), host wall clock"}}
     if not args.no_cpu_baseline:
         try:
             sys.path.insert(0, os.path.join(ROOT, "tests"))
             import oracle_bind
             kind = "fast" if oracle_bind.ref_available("fast") else "strict"
+            t_ref = time.perf_counter()
             ref = oracle_bind.RefScene(G.config_params(3, width=vw, height=vh), freqs=freqs, kind=kind)
+            res["create_ms"]["reference"] = 1e3 * (time.perf_counter() - t_ref)
+            res["create_ms"]["reference_build"] = kind
             stride = 8
             _, secs, threads = ref.render_spectral_rows(0, stride)
             npf = len(range(0, vh, stride)) * vw * nb

@@ -131,6 +131,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_render_rows_device": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]),
         "grrt_tonemap_device": (C.c_int, [vp, C.c_int, C.c_int, vp]),
         "grrt_render_spectral_device": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
+        "grrt_render_spectral_rows_device": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+        "grrt_render_spectral_tile_device": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
         "grrt_render_spectral_device_noalloc": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.c_int, vp]),
         "grrt_get_stats": (C.c_int, [vp, P(GRRTStats)]),
         "grrt_get_phase_ms": (C.c_int, [vp, P(C.c_double), C.c_int]),
@@ -345,6 +347,27 @@ class Renderer:
         s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
         self._check(self._L.grrt_render_spectral_device(self.ctx, ptr(d_spec), width, height, ptr(d_fate), s),
                     "grrt_render_spectral_device")
+
+    def render_spectral_rows_device(self, row0: int, row_step: int, n_rows: int, d_spec, d_fate=None,
+                                    stream=None) -> None:
+        """Spectral render of image rows row0, row0 + row_step, ... (n_rows, full width) into device buffers."""
+        def ptr(x):
+            if x is None:
+                return None
+            return x if isinstance(x, int) else x.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_render_spectral_rows_device(self.ctx, row0, row_step, n_rows, ptr(d_spec),
+                                                             ptr(d_fate), s), "grrt_render_spectral_rows_device")
+
+    def render_spectral_tile_device(self, x: int, y: int, w: int, h: int, d_spec, d_fate=None, stream=None) -> None:
+        """Spectral render of the w x h tile at image pixel (x, y) into device buffers."""
+        def ptr(v):
+            if v is None:
+                return None
+            return v if isinstance(v, int) else v.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_render_spectral_tile_device(self.ctx, x, y, w, h, ptr(d_spec), ptr(d_fate), s),
+                    "grrt_render_spectral_tile_device")
 
     def render_spectral_device_noalloc(self, d_freqs, nb: int, d_spec, width: int, height: int,
                                        stream=None) -> None:

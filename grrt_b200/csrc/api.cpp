@@ -322,6 +322,48 @@ extern "C" GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double*
     return ctx->render_spectral_device(width, height, d_spec, d_fate, static_cast<cudaStream_t>(stream), true);
 }
 
+extern "C" GRRT_EXPORT int grrt_render_spectral_rows_device(GRRTContext* ctx, int row0, int row_step, int n_rows,
+                                                            double* d_spec, unsigned int* d_fate, void* stream) {
+    if (!ctx) return -1;
+    if (ctx->freq_bins.empty()) {
+        ctx->error = "No frequency bins set -- call grrt_set_frequency_bins first";
+        return -1;
+    }
+    if (row0 < 0 || row_step < 1 || n_rows < 1 ||
+        static_cast<long long>(row0) + static_cast<long long>(n_rows - 1) * row_step >= ctx->params.height) {
+        ctx->error = "grrt_render_spectral_rows_device: rows outside the image";
+        return -1;
+    }
+    DevTile tile;
+    tile.y0 = row0;
+    tile.w = ctx->params.width;
+    tile.h = n_rows;
+    tile.out_pitch = ctx->params.width;
+    tile.row_step = row_step;
+    return ctx->render_spectral_tile(tile, d_spec, d_fate, static_cast<cudaStream_t>(stream), true);
+}
+
+extern "C" GRRT_EXPORT int grrt_render_spectral_tile_device(GRRTContext* ctx, int x, int y, int w, int h,
+                                                            double* d_spec, unsigned int* d_fate, void* stream) {
+    if (!ctx) return -1;
+    if (ctx->freq_bins.empty()) {
+        ctx->error = "No frequency bins set -- call grrt_set_frequency_bins first";
+        return -1;
+    }
+    if (x < 0 || y < 0 || w < 1 || h < 1 || static_cast<long long>(x) + w > ctx->params.width ||
+        static_cast<long long>(y) + h > ctx->params.height) {
+        ctx->error = "grrt_render_spectral_tile_device: tile outside the image";
+        return -1;
+    }
+    DevTile tile;
+    tile.x0 = x;
+    tile.y0 = y;
+    tile.w = w;
+    tile.h = h;
+    tile.out_pitch = w;
+    return ctx->render_spectral_tile(tile, d_spec, d_fate, static_cast<cudaStream_t>(stream), true);
+}
+
 extern "C" GRRT_EXPORT int grrt_get_stats(GRRTContext* ctx, GRRTStats* out) {
     if (!ctx || !out) return -1;
     return ctx->read_stats(out);

@@ -505,9 +505,19 @@ int GRRTContext::render_rgb_to_host(const DevTile& tile, float* host, grrt_progr
 
 int GRRTContext::render_spectral_device(int width, int height, double* d_spec, unsigned* d_fate, cudaStream_t s,
                                         bool reset_stats) {
+    DevTile tile;
+    tile.w = width;
+    tile.h = height;
+    tile.out_pitch = width;
+    return render_spectral_tile(tile, d_spec, d_fate, s, reset_stats);
+}
+
+int GRRTContext::render_spectral_tile(const DevTile& tile, double* d_spec, unsigned* d_fate, cudaStream_t s,
+                                      bool reset_stats) {
     if (!ensure_device()) return -1;
     error.clear();
     *reinterpret_cast<volatile int*>(h_cancel) = 0;
+    const int width = tile.w, height = tile.h;
     const int nb = static_cast<int>(freq_bins.size());
     const size_t n = static_cast<size_t>(width) * height * nb;
     if (reset_stats && fail_cuda(cudaMemsetAsync(d_stats, 0, sizeof(DevStats), s), "reset stats")) return -1;
@@ -550,10 +560,6 @@ int GRRTContext::render_spectral_device(int width, int height, double* d_spec, u
         if (fail_cuda(cudaMalloc(&d_spec_scratch, need * sizeof(double)), "cudaMalloc(spectral scratch)")) return -1;
         d_spec_scratch_n = need;
     }
-    DevTile tile;
-    tile.w = width;
-    tile.h = height;
-    tile.out_pitch = width;
     LaunchResources res;
     res.queue = d_queue;
     res.stats = d_stats;

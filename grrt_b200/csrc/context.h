@@ -96,6 +96,8 @@ struct GRRTContext {
     int render_rgb_to_host(const grrt_b200::DevTile& tile, float* host, grrt_progress_fn cb, void* user);
     int render_spectral_device(int width, int height, double* d_spec, unsigned* d_fate, cudaStream_t s,
                                bool reset_stats);
+    int render_spectral_tile(const grrt_b200::DevTile& tile, double* d_spec, unsigned* d_fate, cudaStream_t s,
+                             bool reset_stats);
     int render_spectral_to_host(int width, int height, double* host, grrt_progress_fn cb, void* user);
     int render_spectral_to_fits(const char* path, int width, int height, grrt_progress_fn cb, void* user);
     int read_stats(GRRTStats* out);

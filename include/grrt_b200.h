@@ -95,6 +95,22 @@ GRRT_EXPORT int grrt_tonemap_device(float* d_rgba, int width, int height, void* 
 GRRT_EXPORT int grrt_render_spectral_device(GRRTContext* ctx, double* d_spec, int width, int height,
                                             unsigned int* d_fate, void* stream);
 
+/* The same for the n_rows image rows row0, row0 + row_step, ... at full width,
+ * written densely (output row k = image row row0 + k * row_step; d_spec is
+ * double[n_rows*W*nb], d_fate one word per sample or NULL): a rank's share of
+ * a spectral frame split across GPUs by interleaved rows. Each pixel is
+ * computed exactly as in the full render. -1 when a row lies outside the image
+ * or no bins are set. */
+GRRT_EXPORT int grrt_render_spectral_rows_device(GRRTContext* ctx, int row0, int row_step, int n_rows,
+                                                 double* d_spec, unsigned int* d_fate, void* stream);
+
+/* The same for the w x h tile at image pixel (x, y) (the spectral counterpart
+ * of grrt_render_tile, api.cpp:215-218 in the reference, whose CPU version
+ * is a stub): d_spec is double[w*h*nb], row-major over the tile. -1 when the
+ * tile leaves the image or no bins are set. */
+GRRT_EXPORT int grrt_render_spectral_tile_device(GRRTContext* ctx, int x, int y, int w, int h, double* d_spec,
+                                                 unsigned int* d_fate, void* stream);
+
 /* Spectral render that allocates no device memory. No counterpart in the
  * reference (its renders run on host threads and allocate host buffers).
  *

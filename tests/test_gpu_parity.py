@@ -16,7 +16,7 @@ import math
 import numpy as np
 import pytest
 
-from parity_util import OracleRGB, OracleSpectral, device_render_rgb, device_render_spectral, rel_err
+from parity_util import OracleRGB, OracleSpectral, device_render_rgb, device_render_spectral, hull_error, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -24,6 +24,10 @@ TOL = 1e-9
 LOOSE = 1e-6
 MIN_WITHIN = 0.99
 MAX_BAND = 0.06  # fraction of pixels allowed in the rounding-sensitive band (1 spp)
+# image-integrated flux per frequency bin (band pixels included)
+FLUX_TOL = 1e-6
+# fraction of band pixels allowed outside the oracle's probe range by more than LOOSE
+MAX_BAND_OFF = 0.25
 
 
 def report(R, frac, within, err, out, stats, ocnt):
@@ -33,6 +37,21 @@ def report(R, frac, within, err, out, stats, ocnt):
           f"{within:.5f} within {TOL}, rel-err quantiles 50/90/99/100% {q[0]:.2e} {q[1]:.2e} {q[2]:.2e} "
           f"{q[3]:.2e}; all pixels within {TOL}: {allq:.5f}; attempts gpu {stats['attempts']} oracle "
           f"{ocnt['attempts']}")
+
+
+def check_band(got, orc, band):
+    """Band pixels: each must lie within LOOSE of the range spanned by the
+    oracle and its rounding probes (a pixel whose samples the probes send to
+    different fates can land anywhere in between, or, on a chaotic
+    near-critical orbit, outside it: those are counted and bounded)."""
+    herr = hull_error(got, orc.pixel_lo, orc.pixel_hi)
+    assert np.all(herr[~band] <= LOOSE + 1e-9)  # outside the band the hull holds the 1e-6 bar above
+    n_band = int(band.sum())
+    off = int(np.sum(herr[band] > LOOSE))
+    print(f"  band pixels: {n_band}; outside the probe range by more than {LOOSE}: {off}"
+          + (f" (max {herr[band].max():.2e})" if n_band else ""))
+    assert off <= max(2, int(MAX_BAND_OFF * n_band)), f"{off} of {n_band} band pixels outside the probe range"
+    return off
 
 
 def check_rgb(grrt, R, pix_all: bool = True, n_sample: int = 0, seed: int = 0, max_band=MAX_BAND,
@@ -68,6 +87,7 @@ def check_rgb(grrt, R, pix_all: bool = True, n_sample: int = 0, seed: int = 0, m
     report(R, frac, within, err, out, stats, orc.counters)
     assert within >= MIN_WITHIN, f"only {within:.4%} of pixels outside the band within {TOL}"
     assert worst <= LOOSE, f"max relative error outside the band {worst:.3e}"
+    check_band(got, orc, band)
     # work: same method, so the attempt count matches the oracle's closely
     if pix_all and same_work:
         assert abs(stats["attempts"] - orc.counters["attempts"]) <= 0.01 * orc.counters["attempts"]
@@ -141,6 +161,12 @@ def check_spectral(grrt, R, freqs, pix, max_band):
     report(R, frac, within, err, out, stats, orc.counters)
     assert within >= MIN_WITHIN, f"only {within:.4%} of pixels outside the band within {TOL}"
     assert worst <= LOOSE, f"max relative error outside the band {worst:.3e}"
+    check_band(got, orc, band)
+    # image-integrated flux per bin over every checked pixel, band included
+    fg, fo = got.sum(axis=0), orc.pixel_spec.sum(axis=0)
+    ferr = float(np.max(rel_err(fg, fo, floor=1e-300 + 1e-12 * np.max(np.abs(fo)))))
+    print(f"  integrated flux per bin: max relative error {ferr:.2e}")
+    assert ferr <= FLUX_TOL, f"integrated flux per bin differs by {ferr:.3e}"
     assert stats["bin_updates"] == stats["physics_steps"] * nb
     return frac, worst, stats
 
