@@ -599,6 +599,28 @@ def run_surrogate(args, torch, G, stream, flush, peaks):
     scale = float(b.max())
     rel = (np.abs(a - b) / np.maximum(np.abs(b), 1e-6 * scale)).max(axis=2)
     lit = b.max(axis=2) > 1e-6 * scale
+    fates_fp64 = rfate.cpu().numpy()
+    # Speed against colour error: the colour tolerance tol_rel sets which lit
+    # samples the network shades (those whose calibrated crossing band moves
+    # the colour by at most tol_rel); the rest are re-traced in FP64. Errors
+    # are against the FP64 form, on lit pixels (colour above 1e-6 x the frame
+    # maximum), so they are the network's own errors on the samples it shades.
+    bands0 = S.bands()
+    pareto = []
+    for tol in (1e-3, 3e-3, 1e-2, 3e-2, 1e-1):
+        S.set_bands(bands0["du"], bands0["dir"], bands0["capture"], bands0["graze"], tol)
+        ms_t = timed(lambda: S.render_device(R, None, out, ofate, stream))
+        c_t = S.last_counts()
+        o_t = out.cpu().numpy()
+        rel_t = (np.abs(o_t - b) / np.maximum(np.abs(b), 1e-6 * scale)).max(axis=2)
+        pareto.append({"tol_rel": tol, "ms_per_step": ms_t, "speedup_vs_fp64": ms_fp64 / ms_t,
+                       "exact_fraction": c_t["exact"] / max(1, c_t["samples"]),
+                       "lit_rel_quantiles_50_90_99_100": [float(x) for x in
+                                                          np.quantile(rel_t[lit], [0.5, 0.9, 0.99, 1.0])],
+                       "pixels_over_1e-3": int((rel_t > 1e-3).sum()),
+                       "pixels_over_1e-2": int((rel_t > 1e-2).sum()),
+                       "sample_fates_differing": int(np.sum(ofate.cpu().numpy() != fates_fp64))})
+    S.set_bands(bands0["du"], bands0["dir"], bands0["capture"], bands0["graze"], bands0["tol_rel"])
     mlp_tflops = F_MLP * n * n / (ms_mlp * 1e-3) / 1e12
     peak = peaks.get("bf16_tflops")
     rays = n * n
@@ -622,6 +644,7 @@ def run_surrogate(args, torch, G, stream, flush, peaks):
                           "sample_fates_differing": int((ofate != rfate).sum().item()),
                           "rel_floor": "max(|fp64|, 1e-6 x frame max)"},
         "calibration": cal,
+        "colour_tolerance_pareto": pareto,
         "train": {"seconds": t_train, "generate_seconds": t_gen, "loss_first": float(np.mean(hist[:20])),
                   "loss_last": float(np.mean(hist[-20:])),
                   "samples_per_s": args.surrogate_steps * 16384 / t_train,

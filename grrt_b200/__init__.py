@@ -77,7 +77,7 @@ class GRRTStats(C.Structure):
         ("rays", C.c_ulonglong), ("horizon", C.c_ulonglong), ("escaped", C.c_ulonglong),
         ("max_steps", C.c_ulonglong), ("clamp_evals", C.c_ulonglong), ("march_steps", C.c_ulonglong),
         ("physics_steps", C.c_ulonglong), ("bin_updates", C.c_ulonglong),
-        ("fp64_attempts", C.c_ulonglong), ("kernel_ms", C.c_double),
+        ("fp64_attempts", C.c_ulonglong), ("kernel_ms", C.c_double), ("hamiltonian_max", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -169,6 +169,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_batch_render": (C.c_int, [vp, P(P(C.c_float))]),
         "grrt_batch_render_device": (C.c_int, [vp, vp, vp]),
         "grrt_batch_get_stats": (C.c_int, [vp, P(GRRTStats)]),
+        "grrt_batch_set_frequency_bins": (C.c_int, [vp, C.c_int, P(C.c_double), C.c_int]),
+        "grrt_batch_set_tuning": (C.c_int, [vp, C.c_int, C.c_double, C.c_double]),
+        "grrt_batch_get_tuning": (C.c_int, [vp, P(C.c_int), P(C.c_double), P(C.c_double)]),
+        "grrt_batch_spectral_offset": (C.c_longlong, [vp, C.c_int]),
+        "grrt_batch_render_spectral_device": (C.c_int, [vp, vp, vp]),
+        "grrt_batch_render_spectral": (C.c_int, [vp, P(P(C.c_double))]),
         "grrt_scene_table": (C.c_longlong, [vp, C.c_char_p, P(C.c_double), C.c_longlong]),
         "grrt_camera_ray": (C.c_int, [vp, C.c_double, C.c_double, P(C.c_double)]),
         "grrt_debug_trace": (C.c_int, [vp, C.c_double, C.c_double, P(GRRTDebugRecord), C.c_int]),
@@ -428,23 +434,32 @@ class Renderer:
 
 
 class Batch:
-    """Many thin-disk cameras rendered by one persistent launch (grrt_batch_*)."""
+    """Many cameras rendered by one persistent launch (grrt_batch_*): thin-disk
+    cameras (RGB) or volumetric cameras (spectra, each with its own bins)."""
 
     ORDER_CAMERA_MAJOR = 0
     ORDER_ROUND_ROBIN = 1
 
-    def __init__(self, cameras: Sequence[dict]):
+    def __init__(self, cameras: Sequence[dict], freqs: Optional[Sequence] = None):
+        """freqs: per camera, the bins (Hz) of a volumetric camera or None. As
+        for a Renderer, they widen the camera's opacity tables at creation and
+        become its render bins."""
         self._L = lib()
         self.cameras = [dict(c) for c in cameras]
+        fl = [None if (freqs is None or f is None) else np.ascontiguousarray(f, dtype=np.float64)
+              for f in (freqs if freqs is not None else [None] * len(cameras))]
         arr = (GRRTParams * len(cameras))()
         for i, c in enumerate(cameras):
-            arr[i] = make_params(c)
+            arr[i] = make_params(c, fl[i])
         self.b = self._L.grrt_batch_create(arr, len(cameras))
         if not self.b:
             err = self._L.grrt_batch_error(None)
             raise RuntimeError("grrt_batch_create failed: " + (err.decode() if err else "unknown"))
         self.sizes = [(c["width"], c["height"]) for c in cameras]
         self.offsets = np.cumsum([0] + [w * h for w, h in self.sizes])
+        for i, f in enumerate(fl):
+            if f is not None:
+                self.set_frequency_bins(f, i)
 
     def close(self) -> None:
         if getattr(self, "b", None):
@@ -464,6 +479,37 @@ class Batch:
 
     def set_precision(self, form: int) -> None:
         self._check(self._L.grrt_batch_set_precision(self.b, form), "grrt_batch_set_precision")
+
+    def set_frequency_bins(self, freqs, camera: int = -1) -> None:
+        """Bins (Hz) of one camera, or of every camera (camera = -1)."""
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        self._check(self._L.grrt_batch_set_frequency_bins(self.b, camera, _dptr(f), len(f)),
+                    "grrt_batch_set_frequency_bins")
+
+    def set_tuning(self, block: int = 128, tol_fp32: float = 3e-6, r_factor: float = 3.0) -> None:
+        self._check(self._L.grrt_batch_set_tuning(self.b, block, tol_fp32, r_factor), "grrt_batch_set_tuning")
+
+    def tuning(self) -> dict:
+        a, t, r = C.c_int(), C.c_double(), C.c_double()
+        self._L.grrt_batch_get_tuning(self.b, C.byref(a), C.byref(t), C.byref(r))
+        return {"block": a.value, "tol_fp32": t.value, "r_factor": r.value}
+
+    def spectral_offset(self, camera: int) -> int:
+        """Element offset of camera's cube in the batch's spectral output (camera = count: total size)."""
+        return int(self._L.grrt_batch_spectral_offset(self.b, camera))
+
+    def render_spectral_device(self, d_spec, stream=None) -> None:
+        p = d_spec if isinstance(d_spec, int) else d_spec.data_ptr()
+        s = stream if (stream is None or isinstance(stream, int)) else stream.cuda_stream
+        self._check(self._L.grrt_batch_render_spectral_device(self.b, p, s), "grrt_batch_render_spectral_device")
+
+    def render_spectral(self) -> list:
+        n = len(self.cameras)
+        sizes = [self.spectral_offset(i + 1) - self.spectral_offset(i) for i in range(n)]
+        cubes = [np.empty(k, dtype=np.float64) for k in sizes]
+        ptrs = (C.POINTER(C.c_double) * n)(*[_dptr(c) for c in cubes])
+        self._check(self._L.grrt_batch_render_spectral(self.b, ptrs), "grrt_batch_render_spectral")
+        return [c.reshape(h, w, -1) for c, (w, h) in zip(cubes, self.sizes)]
 
     def set_schedule(self, chunk: int, order: int, blocks_per_sm: int = 0) -> None:
         self._check(self._L.grrt_batch_set_schedule(self.b, chunk, order, blocks_per_sm), "grrt_batch_set_schedule")

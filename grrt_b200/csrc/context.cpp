@@ -698,6 +698,7 @@ int GRRTContext::read_stats(GRRTStats* out) {
     out->physics_steps = s.physics_steps;
     out->bin_updates = s.bin_updates;
     out->fp64_attempts = s.fp64_attempts;
+    std::memcpy(&out->hamiltonian_max, &s.h_max_bits, sizeof(double));
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) out->kernel_ms = ms;
     cudaGetLastError();

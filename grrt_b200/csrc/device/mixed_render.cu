@@ -152,6 +152,15 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 // pass gains more from the fifth block's warps than it loses to the few
 // spilled registers (four blocks: 8.8 ms, five: 8.2 ms on the 1024x1024 4-spp
 // frame on B200; six, with more spills, no better).
+// Warp maximum of the lanes' |H| / p_t^2 into the launch's maximum (the
+// bits of a non-negative double order as integers).
+__device__ __forceinline__ void warp_max_h(DevStats* st, float h) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h = fmaxf(h, __shfl_xor_sync(kMask, h, o));
+    if ((threadIdx.x & 31u) == 0 && h > 0.0f)
+        atomicMax(&st->h_max_bits, static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(h))));
+}
+
 // True on every lane of the warp once the host has raised the cancel flag
 // (a host-mapped word; lane 0 reads it). Callers poll every 1024 loop
 // iterations, as the FP64 kernels do.
@@ -337,6 +346,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
     int retry = 0, step = 0, ncross = 0;
     unsigned iter = 0;
     double c0 = 0, c1 = 0, c2 = 0;
+    float h_max = 0.0f;  // max |H| / p_t^2 at the final state of the lane's samples
     while (true) {
         const bool want = !live && !exhausted;
         const unsigned nq = fetch(want, mb.queue2, total);
@@ -411,6 +421,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
         }
         if (live && term >= 0) {
             live = false;
+            h_max = fmaxf(h_max, static_cast<float>(fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt)));
             if (term == kTermEscaped && S.stars_on) {
                 const double b = star_brightness(S.stars, y.th, y.ph);
                 c0 += b;
@@ -426,6 +437,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
     }
 #undef S
     warp_add(stats, n_att, n_acc, 0ull, n_att);
+    warp_max_h(stats, h_max);
 }
 
 // Per pixel: sum the spp sample colours in order, scale, write the outputs.

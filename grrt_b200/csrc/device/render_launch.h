@@ -148,10 +148,11 @@ int debug_trace_capacity(int max_steps);
 cudaError_t launch_debug_trace(const DevScene& S, double x, double y, DevDebugRecord* rec, int cap, int* count,
                                cudaStream_t stream);
 
-// Batched thin-disk render over many cameras (see DevBatch), FP64 form.
+// Batched thin-disk render over many cameras (see DevBatch), FP64 form, with
+// blocks of `block` threads (64, 128 or 256; the same registers per thread).
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats,
-                              int blocks, cudaStream_t stream);
-int thin_batch_max_blocks_per_sm();
+                              int blocks, int block, cudaStream_t stream);
+int thin_batch_max_blocks_per_sm(int block);
 
 // Batched mixed form: the four phases of launch_thin_mixed, each one launch
 // over the samples of every item (B.n_items, n_samples, n_pixels and each
@@ -162,6 +163,18 @@ cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* o
                                     DevStats* stats, void* scratch, size_t scratch_bytes, int blocks_per_sm,
                                     cudaStream_t stream);
 int mixed_batch_max_blocks_per_sm();
+
+// Batched volumetric spectral render over many cameras, FP64 form: one
+// persistent launch of the warp-cooperative spectral kernel over the batch's
+// chunk table. Each item carries its bins (freqs, nb) and its output offset
+// (spec_offset, in elements); nb_max is the largest nb (the per-lane row
+// stride), scratch holds 4 * nb_max doubles per lane of `blocks` blocks of
+// vol_spectral_batch_threads() threads.
+cudaError_t launch_vol_spectral_batch(const DevBatch& B, int nb_max, double* out_spec, double* scratch,
+                                      size_t scratch_elems, unsigned* queue, DevStats* stats, int blocks,
+                                      cudaStream_t stream);
+int vol_spectral_batch_max_blocks_per_sm();
+int vol_spectral_batch_threads();
 
 // Spectral render whose scratch is a file-scope device array (no allocation);
 // see vol_render.cu. Returns cudaErrorInvalidValue when nb exceeds the limit.

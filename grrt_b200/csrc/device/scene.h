@@ -109,6 +109,11 @@ struct DevBatchItem {
     int out_pitch = 0;           // output row pitch in pixels
     size_t out_offset = 0;       // first output pixel of this item
     size_t sample0 = 0;          // first sample of this item (mixed form: samples of all items in item order)
+    // spectral batches: the item's observer-frame frequencies (device), their
+    // count, and the item's first output element (its cube is [w*h][nb])
+    const double* freqs = nullptr;
+    int nb = 0;
+    size_t spec_offset = 0;
 };
 struct DevBatchChunk {
     int item = 0;
@@ -142,7 +147,10 @@ struct DevStats {
     unsigned long long bin_updates;   // per-frequency transfer updates
     unsigned long long fp64_attempts; // mixed form: attempts taken in FP64
     unsigned long long cancelled;     // launches that observed the cancel flag
-    unsigned long long pad[3];
+    // max over FP64-traced samples of |H| / p_t^2 at the final state, as the
+    // bits of a non-negative double (integer order = value order)
+    unsigned long long h_max_bits;
+    unsigned long long pad[2];
 };
 
 }  // namespace grrt_b200

@@ -39,29 +39,45 @@ constexpr unsigned kFull = 0xffffffffu;
 #define GRRT_THIN_MIN_BLOCKS 4
 #endif
 
-struct LaneCounters {
-    unsigned long long attempts = 0, accepted = 0, crossings = 0, rays = 0;
-    unsigned long long horizon = 0, escaped = 0, maxsteps = 0, fp64_attempts = 0;
+// Per-lane state that is touched only when a sample starts, crosses the disk
+// or ends. It lives in shared memory, so the registers hold the ray itself
+// (state, kept first stage, step size) through the DP45 attempt.
+struct LaneCold {
+    double acc[3];        // the pixel's sum over its finished samples
+    double col[3];        // the current sample's colour (disk crossings, then the star)
+    size_t out;           // output index of the pixel
+    int i, j;             // image coordinates of the pixel
+    int smp;              // sample index within the pixel
+    int ncross;           // the current sample's emitting disk crossings
+    unsigned crossings, horizon, escaped, maxsteps;  // counters of the lane's samples
+    double h_max;         // max |H| / p_t^2 at the final state of the lane's samples
 };
 
-__device__ __forceinline__ void flush_counters(DevStats* st, const LaneCounters& c, bool cancelled) {
-    unsigned long long v[8] = {c.attempts, c.accepted, c.crossings, c.rays,
-                               c.horizon, c.escaped, c.maxsteps, c.fp64_attempts};
+// Sums the lanes' counters per warp and adds them to the launch's totals
+// (every DP45 attempt of this kernel is an FP64 attempt).
+__device__ __forceinline__ void flush_counters(DevStats* st, unsigned attempts, unsigned accepted,
+                                               const LaneCold& c, bool cancelled) {
+    unsigned long long v[6] = {attempts, accepted, c.crossings, c.horizon, c.escaped, c.maxsteps};
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
+    for (int k = 0; k < 6; ++k)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(kFull, v[k], o);
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&st->attempts, v[0]);
         atomicAdd(&st->accepted, v[1]);
         atomicAdd(&st->crossings, v[2]);
-        atomicAdd(&st->rays, v[3]);
-        atomicAdd(&st->horizon, v[4]);
-        atomicAdd(&st->escaped, v[5]);
-        atomicAdd(&st->max_steps, v[6]);
-        atomicAdd(&st->fp64_attempts, v[7]);
+        atomicAdd(&st->rays, v[3] + v[4] + v[5]);
+        atomicAdd(&st->horizon, v[3]);
+        atomicAdd(&st->escaped, v[4]);
+        atomicAdd(&st->max_steps, v[5]);
+        atomicAdd(&st->fp64_attempts, v[0]);
         if (cancelled && threadIdx.x == 0) atomicAdd(&st->cancelled, 1ull);
     }
+    double h = c.h_max;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h = fmax(h, __shfl_xor_sync(kFull, h, o));
+    if ((threadIdx.x & 31) == 0 && h > 0.0)
+        atomicMax(&st->h_max_bits, static_cast<unsigned long long>(__double_as_longlong(h)));
 }
 
 // Start-of-step termination test in the reference order: step budget first
@@ -81,7 +97,7 @@ __device__ __forceinline__ int start_check(const DevScene& S, int step, double r
 // kBatch = true: work index -> (chunk, offset) through the batch's chunk table,
 // so one launch covers many cameras (scenes[item.scene]) in the order the
 // schedule lists the chunks.
-template <bool kBatch>
+template <bool kBatch, int kBlock = kThreads>
 __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B, const DevTile& tile,
                                           float4* __restrict__ out_rgba, double* __restrict__ out_rgb64,
                                           uint32_t* __restrict__ out_fate, unsigned total,
@@ -92,23 +108,22 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
     // the scene of the lane's current pixel (batch: per lane, in global memory)
     int scene = 0;
 #define S (kBatch ? B.scenes[scene] : S0)
-    int px_i = 0, px_j = 0;   // image coordinates of the lane's pixel
-    size_t px_out = 0;        // output index of the lane's pixel
+    __shared__ LaneCold cold_all[kBlock];
+    LaneCold& cold = cold_all[threadIdx.x];
+    cold.crossings = cold.horizon = cold.escaped = cold.maxsteps = 0;
+    cold.h_max = 0.0;
 
-    LaneCounters cnt;
+    unsigned n_attempts = 0, n_accepted = 0;
     // pixel slot
     int pix = -1;        // work index of the lane's pixel; -1 = needs a pixel; -2 = queue exhausted
-    int smp = 0;         // sample index within the pixel
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     // ray slot
     bool live = false;
     Vec5<double> y;      // state at the start of the current outer step
     Vec5<double> k1;     // f(y), kept from the previous attempt when k1_ok
     bool k1_ok = false;
     double pt = 0.0, pph = 0.0;
-    double dl = 0.0, dlambda = 0.0;
-    int retry = 0, step = 0, ncross = 0;
-    double col0 = 0.0, col1 = 0.0, col2 = 0.0;
+    double dl = 0.0;
+    int retry = 0, step = 0;
     bool cancelled = false;
     unsigned iter = 0;
 
@@ -132,21 +147,21 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
                             const int local = ch.start + within;
                             const int qx = local % it.w, qy = local / it.w;
                             scene = it.scene;
-                            px_i = it.x0 + qx;
-                            px_j = it.y0 + qy;
-                            px_out = it.out_offset + static_cast<size_t>(qy) * it.out_pitch + qx;
+                            cold.i = it.x0 + qx;
+                            cold.j = it.y0 + qy;
+                            cold.out = it.out_offset + static_cast<size_t>(qy) * it.out_pitch + qx;
                             pix = static_cast<int>(q);
-                            smp = 0;
-                            acc0 = acc1 = acc2 = 0.0;
+                            cold.smp = 0;
+                            cold.acc[0] = cold.acc[1] = cold.acc[2] = 0.0;
                         }  // else: padding slot of a short chunk, fetch again
                     } else {
                         const int qx = static_cast<int>(q) % tile.w, qy = static_cast<int>(q) / tile.w;
-                        px_i = tile.x0 + qx;
-                        px_j = tile.y0 + qy * tile.row_step;
-                        px_out = static_cast<size_t>(qy) * tile.out_pitch + qx;
+                        cold.i = tile.x0 + qx;
+                        cold.j = tile.y0 + qy * tile.row_step;
+                        cold.out = static_cast<size_t>(qy) * tile.out_pitch + qx;
                         pix = static_cast<int>(q);
-                        smp = 0;
-                        acc0 = acc1 = acc2 = 0.0;
+                        cold.smp = 0;
+                        cold.acc[0] = cold.acc[1] = cold.acc[2] = 0.0;
                     }
                 } else {
                     pix = -2;
@@ -155,7 +170,7 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
         }
         // ---- start a ray for lanes that have a pixel but no live ray ----
         if (!live && pix >= 0) {
-            const int i = px_i, j = px_j;
+            const int i = cold.i, j = cold.j, smp = cold.smp;
             const int sy = smp / S.grid, sx = smp % S.grid;
             const double x = i + (sx + pixel_hash(i, j, smp, 0)) * S.cell;
             const double yy = j + (sy + pixel_hash(i, j, smp, 1)) * S.cell;
@@ -164,12 +179,11 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
             y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], p[1], p[2]};
             pt = p[0];
             pph = p[3];
-            dlambda = S.dl0;
-            dl = dlambda;
+            dl = S.dl0;
             retry = 0;
             step = 0;
-            ncross = 0;
-            col0 = col1 = col2 = 0.0;
+            cold.ncross = 0;
+            cold.col[0] = cold.col[1] = cold.col[2] = 0.0;
             k1_ok = false;
             live = true;
         }
@@ -184,11 +198,10 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
             }
             Vec5<double> y5, k7;
             const double err = dp45_attempt_k1<double>(S.M, S.a, pt, pph, y, dl, k1, y5, k7);
-            ++cnt.fp64_attempts;
-            ++cnt.attempts;
+            ++n_attempts;
             const StepDecision d = pi_control(err, S.tol, dl, retry, y5.r);
             if (d.accept) {
-                ++cnt.accepted;
+                ++n_accepted;
                 // equatorial crossing (src/geodesic_tracer.cpp:156-176): every
                 // crossing inside the disk adds emission; r is interpolated
                 // linearly in theta; p_t and p_phi are constants of motion.
@@ -201,18 +214,17 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
                         if (rc >= S.r_in && rc <= S.r_out) {
                             double e0, e1, e2;
                             disk_emission(S, rc, pt, pph, e0, e1, e2);
-                            col0 += e0;
-                            col1 += e1;
-                            col2 += e2;
-                            ++ncross;
-                            ++cnt.crossings;
+                            cold.col[0] += e0;
+                            cold.col[1] += e1;
+                            cold.col[2] += e2;
+                            ++cold.ncross;
+                            ++cold.crossings;
                         }
                     }
                 }
                 y = y5;
                 k1 = k7;
-                dlambda = d.next;
-                dl = dlambda;
+                dl = d.next;
                 retry = 0;
                 ++step;
                 term = start_check(S, step, y.r);
@@ -225,30 +237,31 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
         // ---- finish a terminated sample ----
         if (live && term >= 0) {
             live = false;
-            ++cnt.rays;
+            cold.h_max = fmax(cold.h_max, fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt));
+            double c0 = cold.col[0], c1 = cold.col[1], c2 = cold.col[2];
             if (term == kTermEscaped) {
-                ++cnt.escaped;
+                ++cold.escaped;
                 if (S.stars_on) {
                     const double b = star_brightness(S.stars, y.th, y.ph);
-                    col0 += b;
-                    col1 += b;
-                    col2 += b;
+                    c0 += b;
+                    c1 += b;
+                    c2 += b;
                 }
             } else if (term == kTermHorizon) {
-                ++cnt.horizon;
+                ++cold.horizon;
             } else {
-                ++cnt.maxsteps;
+                ++cold.maxsteps;
             }
-            acc0 = acc0 + col0;
-            acc1 = acc1 + col1;
-            acc2 = acc2 + col2;
+            const double acc0 = cold.acc[0] + c0, acc1 = cold.acc[1] + c1, acc2 = cold.acc[2] + c2;
             const int grid2 = S.grid * S.grid;
+            const int smp = cold.smp;
             if (out_fate) {
+                const int ncross = cold.ncross;
                 const unsigned nc = (ncross > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(ncross);
                 out_fate[static_cast<size_t>(pix) * grid2 + smp] = static_cast<unsigned>(term) | (nc << 2);
             }
-            if (++smp == grid2) {
-                const size_t o = px_out;
+            if (smp + 1 == grid2) {
+                const size_t o = cold.out;
                 const double r0 = acc0 * S.inv_spp, r1 = acc1 * S.inv_spp, r2 = acc2 * S.inv_spp;
                 if (out_rgba) out_rgba[o] = make_float4(static_cast<float>(r0), static_cast<float>(r1),
                                                          static_cast<float>(r2), 1.0f);
@@ -258,6 +271,11 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
                     out_rgb64[3 * o + 2] = r2;
                 }
                 pix = -1;
+            } else {
+                cold.smp = smp + 1;
+                cold.acc[0] = acc0;
+                cold.acc[1] = acc1;
+                cold.acc[2] = acc2;
             }
         }
 
@@ -275,7 +293,7 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
         if (!__any_sync(kFull, live || pix >= -1)) break;
     }
 #undef S
-    flush_counters(stats, cnt, cancelled);
+    flush_counters(stats, n_attempts, n_accepted, cold, cancelled);
 }
 
 __global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
@@ -288,12 +306,15 @@ thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float
 }
 
 // One launch over many cameras: the batched form. Work index space =
-// n_chunks * chunk_size (short chunks padded).
-__global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
+// n_chunks * chunk_size (short chunks padded). Instantiated for 64-, 128- and
+// 256-thread blocks at the same register budget (128 per thread); the
+// batch's autotuner picks one.
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock, GRRT_THIN_MIN_BLOCKS * kThreads / kBlock)
 thin_batch_kernel(const __grid_constant__ DevBatch B, float4* __restrict__ out_rgba, unsigned int* __restrict__ queue,
                   DevStats* __restrict__ stats) {
     const unsigned total = static_cast<unsigned>(B.n_chunks) * static_cast<unsigned>(B.chunk_size);
-    thin_loop<true>(B.scenes[0], B, DevTile{}, out_rgba, nullptr, nullptr, total, queue, stats, nullptr);
+    thin_loop<true, kBlock>(B.scenes[0], B, DevTile{}, out_rgba, nullptr, nullptr, total, queue, stats, nullptr);
 }
 
 cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
@@ -321,18 +342,35 @@ cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutput
     return cudaGetLastError();
 }
 
-int thin_batch_max_blocks_per_sm() {
-    int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel, kThreads, 0);
-    return n < 1 ? 1 : n;
+namespace {
+template <int kBlock>
+int thin_batch_blocks_per_sm_for() {
+    return per_device_shape<int>([](int) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, thin_batch_kernel<kBlock>, kBlock, 0);
+        return n < 1 ? 1 : n;
+    });
+}
+}  // namespace
+
+int thin_batch_max_blocks_per_sm(int block) {
+    return block == 64 ? thin_batch_blocks_per_sm_for<64>()
+           : block == 256 ? thin_batch_blocks_per_sm_for<256>()
+                          : thin_batch_blocks_per_sm_for<128>();
 }
 
 cudaError_t launch_thin_batch(const DevBatch& B, float4* out_rgba, unsigned int* queue, DevStats* stats, int blocks,
-                              cudaStream_t stream) {
+                              int block, cudaStream_t stream) {
     if (B.n_chunks <= 0) return cudaSuccess;
+    if (block != 64 && block != 128 && block != 256) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    thin_batch_kernel<<<blocks, kThreads, 0, stream>>>(B, out_rgba, queue, stats);
+    if (block == 64)
+        thin_batch_kernel<64><<<blocks, 64, 0, stream>>>(B, out_rgba, queue, stats);
+    else if (block == 256)
+        thin_batch_kernel<256><<<blocks, 256, 0, stream>>>(B, out_rgba, queue, stats);
+    else
+        thin_batch_kernel<128><<<blocks, 128, 0, stream>>>(B, out_rgba, queue, stats);
     return cudaGetLastError();
 }
 

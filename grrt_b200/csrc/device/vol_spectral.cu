@@ -58,24 +58,40 @@ constexpr unsigned kWarp = 0xffffffffu;
 // written. kList = true: work item k = sample list[k] (pixel * grid^2 + s)
 // of the tile; out_spec[sample][nb] receives the sample's J (its term of the
 // pixel sum is J nu^3).
-template <bool kList>
+// kBatch = true (with kList = false): the batched form over many volumetric
+// cameras. Work index -> (chunk, offset) through the batch's chunk table, as
+// in the thin-disk batch; each lane reads its camera's scene, bins and output
+// offset from the batch's items, and a served lane's bins are those of its
+// own camera. nb is then the largest bin count of the batch (the row stride);
+// tile, freqs and out_fate are unused.
+template <bool kList, bool kBatch = false>
 __global__ void __launch_bounds__(kSpecThreads)
-vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, const double* __restrict__ freqs,
-                    int nb, double* __restrict__ out_spec, uint32_t* __restrict__ out_fate,
+vol_spectral_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const double* __restrict__ freqs0,
+                    int nb0, double* __restrict__ out_spec, uint32_t* __restrict__ out_fate,
                     double* __restrict__ scratch, unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
                     const volatile int* __restrict__ cancel, const unsigned* __restrict__ list,
-                    const unsigned* __restrict__ list_count) {
-    const DevVolume& V = S.vol;
+                    const unsigned* __restrict__ list_count, const __grid_constant__ DevBatch B) {
+    static_assert(!(kList && kBatch), "the batched form has no list mode");
+    // the scene of the lane's current pixel (batch: per lane, in global memory)
+    const DevScene* sp = &S0;
+#define S (kBatch ? *sp : S0)
+#define V (S.vol)
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const int grid2 = S.grid * S.grid;
-    const unsigned total = kList ? *list_count : static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
+    const unsigned total = kList ? *list_count
+                                 : kBatch ? static_cast<unsigned>(B.n_chunks) * static_cast<unsigned>(B.chunk_size)
+                                          : static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
     const size_t slot = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    const size_t row_len = 4 * static_cast<size_t>(nb);
+    // a row is [J | T | tau | pixel sum], each part `seg` doubles
+    const int seg = nb0;
+    const size_t row_len = 4 * static_cast<size_t>(seg);
     // row of lane `src` of this warp: lane slots of a warp are consecutive
     double* const my_row = scratch + slot * row_len;
     auto row_of = [&](int src) { return my_row + (static_cast<ptrdiff_t>(src) - lane) * static_cast<ptrdiff_t>(row_len); };
-    const int med = nb / 2;
+    // the lane's camera (batch): its item, bins and bin count
+    int item = 0;
+    int nb = nb0;
+    const double* freqs = freqs0;
 
     VolCounters cnt;
     int pix = -1, smp = 0;  // kList: pix = the listed sample
@@ -104,9 +120,24 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             if (want) {
                 const unsigned k = base + __popc(want_mask & lt_mask);
                 if (k < total) {
-                    pix = static_cast<int>(kList ? list[k] : k);
-                    smp = 0;
-                    fresh_pixel = true;
+                    if (kBatch) {
+                        const DevBatchChunk ch = B.chunks[k / B.chunk_size];
+                        const int within = static_cast<int>(k % B.chunk_size);
+                        if (within < ch.count) {
+                            item = ch.item;
+                            const DevBatchItem& it = B.items[item];
+                            sp = B.scenes + it.scene;
+                            nb = it.nb;
+                            freqs = it.freqs;
+                            pix = ch.start + within;
+                            smp = 0;
+                            fresh_pixel = true;
+                        }  // else: padding slot of a short chunk, fetch again
+                    } else {
+                        pix = static_cast<int>(kList ? list[k] : k);
+                        smp = 0;
+                        fresh_pixel = true;
+                    }
                 } else {
                     pix = -2;
                 }
@@ -114,10 +145,19 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
         }
         bool fresh_ray = false;
         if (!live && pix >= 0) {
+            const int grid2 = S.grid * S.grid;
             const int pixel = kList ? pix / grid2 : pix;
             const int s = kList ? pix % grid2 : smp;
-            const int qx = pixel % tile.w, qy = pixel / tile.w;
-            const int i = tile.x0 + qx, j = tile.y0 + qy * tile.row_step;
+            int i, j;
+            if (kBatch) {
+                const DevBatchItem& it = B.items[item];
+                i = it.x0 + pixel % it.w;
+                j = it.y0 + pixel / it.w;
+            } else {
+                const int qx = pixel % tile.w, qy = pixel / tile.w;
+                i = tile.x0 + qx;
+                j = tile.y0 + qy * tile.row_step;
+            }
             const int sy = s / S.grid, sx = s % S.grid;
             const double x = i + (sx + pixel_hash(i, j, s, 0)) * S.cell;
             const double yy = j + (sy + pixel_hash(i, j, s, 1)) * S.cell;
@@ -144,11 +184,12 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
                 const int src = __ffs(m) - 1;
                 double* row = row_of(src);
                 const bool new_pixel = !kList && ((pm >> src) & 1u);
-                for (int b = lane; b < nb; b += 32) {
+                const int snb = kBatch ? __shfl_sync(kWarp, nb, src) : nb;
+                for (int b = lane; b < snb; b += 32) {
                     row[b] = 0.0;
-                    row[nb + b] = 1.0;
-                    row[2 * nb + b] = 0.0;
-                    if (new_pixel) row[3 * nb + b] = 0.0;
+                    row[seg + b] = 1.0;
+                    row[2 * seg + b] = 0.0;
+                    if (new_pixel) row[3 * seg + b] = 0.0;
                 }
             }
         }
@@ -267,32 +308,38 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
                 const double fT = __shfl_sync(kWarp, ph_fT, src);
                 const int ir = __shfl_sync(kWarp, ph_ir, src);
                 const int iT = __shfl_sync(kWarp, ph_iT, src);
+                // the served lane's camera: its opacity tables and bins
+                const int sitem = kBatch ? __shfl_sync(kWarp, item, src) : 0;
+                const DevVolume& Vs = kBatch ? B.scenes[B.items[sitem].scene].vol : S0.vol;
+                const double* sfreqs = kBatch ? B.items[sitem].freqs : freqs0;
+                const int snb = kBatch ? B.items[sitem].nb : nb0;
+                const int smed = snb / 2;
                 double* row = row_of(src);
                 double kam = 0.0;
                 int thick = 0;
-                for (int b0 = 0; b0 < nb; b0 += 32) {
+                for (int b0 = 0; b0 < snb; b0 += 32) {
                     const int b = b0 + lane;
                     double ka = 0.0;
                     bool thk = false;
-                    if (b < nb) {
-                        const double nu = ag * __ldg(freqs + b);
-                        ka = v_kappa_abs(V, nu, ir, fr, iT, fT);
+                    if (b < snb) {
+                        const double nu = ag * __ldg(sfreqs + b);
+                        ka = v_kappa_abs(Vs, nu, ir, fr, iT, fT);
                         const double kt = ka + ke;
                         const double eps = (kt > 0.0) ? ka / kt : 1.0;
                         const double dtau = kt * rho * dsp;
-                        const double B = planck_nu(nu, Tl);
-                        const double Sv = eps * B / (nu * nu * nu);
+                        const double B_nu = planck_nu(nu, Tl);
+                        const double Sv = eps * B_nu / (nu * nu * nu);
                         const double e = exp(-dtau);
-                        double tau = row[2 * nb + b];
+                        double tau = row[2 * seg + b];
                         tau += dtau;
-                        row[2 * nb + b] = tau;
+                        row[2 * seg + b] = tau;
                         thk = !(tau <= 10.0);
-                        const double Tb = row[nb + b];
+                        const double Tb = row[seg + b];
                         row[b] += Tb * Sv * (1.0 - e);
-                        row[nb + b] = Tb * e;
+                        row[seg + b] = Tb * e;
                     }
                     thick += __popc(__ballot_sync(kWarp, thk));
-                    if (med >= b0 && med < b0 + 32) kam = __shfl_sync(kWarp, ka, med - b0);
+                    if (smed >= b0 && smed < b0 + 32) kam = __shfl_sync(kWarp, ka, smed - b0);
                 }
                 if (lane == src) {
                     ph_kamed = kam;
@@ -320,7 +367,7 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
 
         // ---- finish a terminated sample ----
         bool finish = false, pixel_done = false;
-        size_t out_row = 0;
+        size_t out_elem = 0;  // first output element of the finished pixel (list: sample)
         if (live && term >= 0) {
             live = false;
             finish = true;
@@ -328,18 +375,23 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             if (term == kTermEscaped) ++cnt.escaped;
             else if (term == kTermHorizon) ++cnt.horizon;
             else ++cnt.maxsteps;
-            if (out_fate) {
+            const int grid2 = S.grid * S.grid;
+            if (!kBatch && out_fate) {
                 const unsigned ne = (entries > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(entries);
                 const size_t q = kList ? static_cast<size_t>(pix) : static_cast<size_t>(pix) * grid2 + smp;
                 out_fate[q] = static_cast<unsigned>(term) | (ne << 2);
             }
             if (kList) {
-                out_row = static_cast<size_t>(pix);
+                out_elem = static_cast<size_t>(pix) * nb;
                 pixel_done = true;
                 pix = -1;
             } else if (++smp == grid2) {
-                const int qx = pix % tile.w, qy = pix / tile.w;
-                out_row = static_cast<size_t>(qy) * tile.out_pitch + qx;
+                if (kBatch) {
+                    out_elem = B.items[item].spec_offset + static_cast<size_t>(pix) * nb;
+                } else {
+                    const int qx = pix % tile.w, qy = pix / tile.w;
+                    out_elem = (static_cast<size_t>(qy) * tile.out_pitch + qx) * nb;
+                }
                 pixel_done = true;
                 pix = -1;
             }
@@ -350,19 +402,23 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
             const unsigned dm = __ballot_sync(kWarp, pixel_done);
             for (unsigned m = fm; m; m &= m - 1) {
                 const int src = __ffs(m) - 1;
-                const size_t o = __shfl_sync(kWarp, static_cast<unsigned long long>(out_row), src);
+                const size_t o = __shfl_sync(kWarp, static_cast<unsigned long long>(out_elem), src);
                 double* row = row_of(src);
                 const bool done = (dm >> src) & 1u;
-                double* dst = out_spec + o * nb;
-                for (int b = lane; b < nb; b += 32) {
+                const int sitem = kBatch ? __shfl_sync(kWarp, item, src) : 0;
+                const double* sfreqs = kBatch ? B.items[sitem].freqs : freqs0;
+                const int snb = kBatch ? B.items[sitem].nb : nb0;
+                const double inv_spp = kBatch ? B.scenes[B.items[sitem].scene].inv_spp : S0.inv_spp;
+                double* dst = out_spec + o;
+                for (int b = lane; b < snb; b += 32) {
                     if (kList) {
                         dst[b] = row[b];  // the sample's J; the resolve forms the sum
                     } else {
-                        const double sum = add_intensity(row[3 * nb + b], row[b], __ldg(freqs + b));
+                        const double sum = add_intensity(row[3 * seg + b], row[b], __ldg(sfreqs + b));
                         if (done)
-                            dst[b] = __dmul_rn(sum, S.inv_spp);
+                            dst[b] = __dmul_rn(sum, inv_spp);
                         else
-                            row[3 * nb + b] = sum;
+                            row[3 * seg + b] = sum;
                     }
                 }
             }
@@ -379,6 +435,8 @@ vol_spectral_kernel(const __grid_constant__ DevScene S, const DevTile tile, cons
         }
         if (!__any_sync(kWarp, live || pix >= -1)) break;
     }
+#undef S
+#undef V
     flush_vol(stats, cnt, cancelled);
 }
 
@@ -637,7 +695,8 @@ cudaError_t launch_vol_spectral_on(const DevScene& S, const DevTile& tile, const
                                    double* out_spec, uint32_t* out_fate, double* scratch, unsigned* queue,
                                    DevStats* stats, const volatile int* cancel, int blocks, cudaStream_t stream) {
     vol_spectral_kernel<false><<<blocks, kSpecThreads, 0, stream>>>(S, tile, freqs, nb, out_spec, out_fate, scratch,
-                                                                     queue, stats, cancel, nullptr, nullptr);
+                                                                     queue, stats, cancel, nullptr, nullptr,
+                                                                     DevBatch{});
     return cudaGetLastError();
 }
 
@@ -655,6 +714,29 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
     if (e != cudaSuccess) return e;
     return launch_vol_spectral_on(S, tile, freqs, nb, out.spec, out.fate, res.spectral_scratch, res.queue, res.stats,
                                   res.cancel, blocks, stream);
+}
+
+int vol_spectral_batch_max_blocks_per_sm() {
+    return per_device_shape<int>([](int) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vol_spectral_kernel<false, true>, kSpecThreads, 0);
+        return n < 1 ? 1 : n;
+    });
+}
+
+int vol_spectral_batch_threads() { return kSpecThreads; }
+
+cudaError_t launch_vol_spectral_batch(const DevBatch& B, int nb_max, double* out_spec, double* scratch,
+                                      size_t scratch_elems, unsigned* queue, DevStats* stats, int blocks,
+                                      cudaStream_t stream) {
+    if (B.n_chunks <= 0) return cudaSuccess;
+    if (nb_max < 1 || !scratch || scratch_elems < static_cast<size_t>(4) * nb_max * blocks * kSpecThreads)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    vol_spectral_kernel<false, true><<<blocks, kSpecThreads, 0, stream>>>(
+        DevScene{}, DevTile{}, nullptr, nb_max, out_spec, nullptr, scratch, queue, stats, nullptr, nullptr, nullptr, B);
+    return cudaGetLastError();
 }
 
 size_t volume_mixed_scratch_bytes(const DevTile& tile, int g2, int nb) {
@@ -710,7 +792,7 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     mark(1);
     vol_spectral_kernel<true><<<lb, kSpecThreads, 0, stream>>>(S, tile, freqs, nb, sample_spec, out.fate,
                                                                 res.spectral_scratch, queue2, res.stats, res.cancel,
-                                                                list, list_count);
+                                                                list, list_count, DevBatch{});
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     mark(2);

@@ -47,6 +47,10 @@ typedef struct {
     unsigned long long bin_updates;   /* per-frequency transfer updates */
     unsigned long long fp64_attempts; /* attempts evaluated in FP64 */
     double kernel_ms;                 /* device time of the render kernels (CUDA events) */
+    double hamiltonian_max;           /* thin-disk FP64 traces (FP64 form, the mixed form's
+                                         re-trace): max over samples of |H| / p_t^2 at the final
+                                         state, H = 1/2 g^{mu nu} p_mu p_nu (0 on the light cone);
+                                         0 where not measured */
 } GRRTStats;
 
 /* Select the precision form for later renders (src/geodesic_tracer.cpp:100 is
@@ -141,7 +145,9 @@ GRRT_EXPORT int grrt_render_spectral_device_noalloc(GRRTContext* ctx, const doub
  * per-camera semantics exactly (tables, jitter, spp). All pixels of all
  * cameras go through one device work queue, so long rays of one camera
  * overlap with short rays of the others; the launch is replayed as a CUDA
- * graph. Volumetric cameras are rejected. */
+ * graph. A batch holds either thin-disk cameras (RGB renders, FP64 or mixed
+ * form) or volumetric cameras (spectral renders, FP64 form; each camera with
+ * its own frequency bins), not both. */
 typedef struct GRRTBatch GRRTBatch;
 
 /* Chunk orders of the schedule: all chunks of camera 0, then camera 1, ...;
@@ -158,9 +164,19 @@ GRRT_EXPORT int grrt_batch_set_precision(GRRTBatch* batch, int form);
  * blocks_per_sm 0 = as many as fit. */
 GRRT_EXPORT int grrt_batch_set_schedule(GRRTBatch* batch, int chunk_size, int order, int blocks_per_sm);
 GRRT_EXPORT int grrt_batch_get_schedule(const GRRTBatch* batch, int* chunk_size, int* order, int* blocks_per_sm);
-/* Times candidate schedules (chunk 64..4096, both orders, two occupancies) and
- * keeps the fastest; cache_path (may be NULL) stores and reuses the choice for
- * an identical batch. best_ms may be NULL. */
+/* Threads per block of the FP64 thin-disk batch kernel (64, 128 or 256, at the
+ * same 128 registers per thread) and the mixed form's FP32 tolerance and
+ * r_factor (as grrt_set_mixed_params) for every camera. Defaults 128, 3e-6, 3. */
+GRRT_EXPORT int grrt_batch_set_tuning(GRRTBatch* batch, int block, double tol_fp32, double r_factor);
+GRRT_EXPORT int grrt_batch_get_tuning(const GRRTBatch* batch, int* block, double* tol_fp32, double* r_factor);
+/* Times candidate settings on the batch itself and keeps the fastest:
+ * FP64 thin-disk batches: chunk 64..4096 x both orders x two occupancies, then
+ * 64/128/256 threads per block; spectral batches: chunk x order x occupancy;
+ * mixed batches: two occupancies x tol_fp32 {1e-6, 3e-6, 1e-5} x r_factor
+ * {3, 4}, each candidate held to the mixed form's bar against the batch's
+ * FP64 render (every pixel within 1e-4 relative) and dropped if it misses it.
+ * cache_path (may be NULL) stores and reuses the choice for an identical
+ * batch. best_ms may be NULL. */
 GRRT_EXPORT int grrt_batch_autotune(GRRTBatch* batch, const char* cache_path, double* best_ms);
 /* framebuffers[i]: float[W_i*H_i*4] host buffer of camera i (NULL skips it). */
 GRRT_EXPORT int grrt_batch_render(GRRTBatch* batch, float* const* framebuffers);
@@ -168,6 +184,21 @@ GRRT_EXPORT int grrt_batch_render(GRRTBatch* batch, float* const* framebuffers);
  * offset sum_{k<i} W_k*H_k. Enqueued on stream. */
 GRRT_EXPORT int grrt_batch_render_device(GRRTBatch* batch, float* d_rgba, void* stream);
 GRRT_EXPORT int grrt_batch_get_stats(GRRTBatch* batch, GRRTStats* out);
+
+/* Volumetric batches. Bins (observer-frame Hz) of one camera, or of every
+ * camera with camera = -1; each camera needs bins before the first render
+ * (as grrt_set_frequency_bins for one context). */
+GRRT_EXPORT int grrt_batch_set_frequency_bins(GRRTBatch* batch, int camera, const double* frequencies_hz,
+                                              int num_bins);
+/* Element offset of camera i's cube in the batch output (i = count gives the
+ * total size); -1 for a thin-disk batch. */
+GRRT_EXPORT long long grrt_batch_spectral_offset(GRRTBatch* batch, int camera);
+/* d_spec: device doubles, camera i's cube double[W_i*H_i*nb_i] (index
+ * (j*W_i + x)*nb_i + k, as grrt_render_spectral) at grrt_batch_spectral_offset(i).
+ * Each camera's cube is bit-identical to its own grrt_render_spectral_device. */
+GRRT_EXPORT int grrt_batch_render_spectral_device(GRRTBatch* batch, double* d_spec, void* stream);
+/* cubes[i]: double[W_i*H_i*nb_i] host buffer of camera i (NULL skips it). */
+GRRT_EXPORT int grrt_batch_render_spectral(GRRTBatch* batch, double* const* cubes);
 
 /* Counters of the last render; synchronises the context's device. */
 GRRT_EXPORT int grrt_get_stats(GRRTContext* ctx, GRRTStats* out);

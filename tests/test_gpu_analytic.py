@@ -49,3 +49,53 @@ def test_schwarzschild_shadow_edge(grrt, need_gpu):
     assert edge_out - edge_in < 0.2 * pix
     # the README's formula lies within one pixel
     assert abs(math.asin(3 * math.sqrt(3) * M / r_obs) - psi_c) < pix
+
+
+def hamiltonian_np(M, a, fin):
+    """H = 1/2 g^{mu nu} p_mu p_nu of Boyer-Lindquist states (t, r, theta,
+    phi, p_t, p_r, p_theta, p_phi), in the separable Kerr form."""
+    r, th = fin[:, 1], fin[:, 2]
+    pt, pr, pth, pph = fin[:, 4], fin[:, 5], fin[:, 6], fin[:, 7]
+    s, c = np.sin(th), np.cos(th)
+    s = np.where(np.abs(s) < 1e-10, np.where(s >= 0, 1e-10, -1e-10), s)
+    sig = r * r + a * a * c * c
+    dlt = r * r - 2 * M * r + a * a
+    P = (r * r + a * a) * pt + a * pph
+    Q = a * s * pt + pph / s
+    return (dlt * pr * pr - P * P / dlt + pth * pth + Q * Q) / (2 * sig)
+
+
+def test_hamiltonian_constraint(grrt, need_gpu):
+    """|H| / p_t^2 at every sample's final state stays near 0 (README.md:213;
+    the reference's CUDA tests hold |H| < 1e-7 along a geodesic,
+    cuda/tests/test_cuda.cu:385-402). The device reports the maximum over the
+    frame (GRRTStats.hamiltonian_max); the oracle's final states of the same
+    samples give the same order of magnitude. Camera rays start null to 1e-10
+    (the reference's camera test)."""
+    import torch
+    from parity_util import OracleRGB
+
+    W = H = 128
+    R = grrt.Renderer(grrt.config_params(2, width=W, height=H, spp=1))  # Kerr a=0.998, stars
+    rgb = torch.empty((H, W, 3), dtype=torch.float64, device="cuda")
+    R.render_device(None, rgb, None)
+    torch.cuda.synchronize()
+    h_dev = R.stats()["hamiltonian_max"]
+    orc = OracleRGB(R, np.arange(W * H), 1e-9, band=False)
+    M, a = R.table("scalars")[:2]
+    h_orc = np.abs(hamiltonian_np(M, a, orc.fin)) / orc.fin[:, 4] ** 2
+    print(f"\n  max |H|/p_t^2 at the final states: device {h_dev:.3e}, oracle {h_orc.max():.3e} "
+          f"(oracle median {np.median(h_orc):.3e})")
+    assert 0.0 < h_dev < 1e-7
+    assert h_dev < 100.0 * h_orc.max() + 1e-12 and h_orc.max() < 100.0 * h_dev + 1e-12
+    # camera rays are null
+    px, py = oracle_bind.jittered_samples(W, H, 1, np.arange(0, W * H, 97))
+    cam = np.array([R.camera_ray(x, y) for x, y in zip(px, py)])
+    h_cam = np.abs(hamiltonian_np(M, a, cam)) / cam[:, 4] ** 2
+    assert h_cam.max() < 1e-10, h_cam.max()
+    # the mixed form's FP64 re-trace reports the same statistic for its samples
+    R.set_precision(grrt.FORM_MIXED)
+    R.render_device(None, rgb, None)
+    torch.cuda.synchronize()
+    h_mix = R.stats()["hamiltonian_max"]
+    assert 0.0 < h_mix <= 1.0001 * h_dev
