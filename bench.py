@@ -15,7 +15,12 @@ generated from its parameters; no dataset).
 The line also carries "surrogate": the learned form, trained in the same run
 on the 64-camera sweep and timed on its evaluation frame (Kerr a=0.998, 80
 deg, 2048^2, 1 spp, thin disk, black background) beside the FP64 and mixed
-forms of that frame (--surrogate-steps 0 skips it).
+forms of that frame, with its colour-tolerance Pareto (--surrogate-steps 0
+skips it); "volumetric": the spectral render (Kerr a=0.9, 512^2, 32 bins) in
+both forms, its FITS output time and the context creation time
+(--no-volumetric skips it); and "batch": the 64-camera sweep in one
+persistent launch, mixed and FP64 forms, against 64 separate launches
+(--no-batch-section skips it).
 
 `value` is rays/s of the headline form (default: mixed, whose output is held
 to <=1e-4 relative of the FP64 form and reported against it) with the scene
@@ -79,6 +84,8 @@ def parse():
     ap.add_argument("--height", type=int, default=1024)
     # the batched sweep (64 cameras, one persistent launch) instead of the headline frame
     ap.add_argument("--batch", action="store_true")
+    # the default line also carries the batched sweep (mixed and FP64 forms); this skips it
+    ap.add_argument("--no-batch-section", action="store_true")
     # the learned surrogate (trained in this run) on its evaluation frame; 0 skips it
     ap.add_argument("--surrogate-steps", type=int, default=20000)
     ap.add_argument("--surrogate-size", type=int, default=2048)
@@ -228,103 +235,100 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_batch(args):
+def batch_section(args, torch, G, stream, flush, form_name="mixed"):
     """Batched sweep: spins {0 (Schwarzschild), 0.5, 0.9, 0.998} x 16 inclinations
     5..90 deg, 256x256 each, thin disk ISCO..20 M, stars seed 42, tolerance 1e-8:
-    one persistent launch (CUDA graph, autotuned schedule) against 64 separate
-    single-camera launches of the same cameras."""
-    import torch
-    import grrt_b200 as G
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    form = G.FORM_MIXED if args.form == "mixed" else G.FORM_FP64
+    one persistent launch (CUDA graph, autotuned schedule and thresholds)
+    against 64 separate single-camera launches of the same cameras; in the
+    mixed form also the FP64 batch and the mixed images' error against it."""
+    form = G.FORM_MIXED if form_name == "mixed" else G.FORM_FP64
     cams = G.sweep_cameras()
     rays = sum(c["width"] * c["height"] for c in cams)
-    B = G.Batch(cams)
-    B.set_precision(form)
     cache = os.path.join(ROOT, "_build", "batch_schedule_cache.jsonl")
     os.makedirs(os.path.dirname(cache), exist_ok=True)
-    tuned_ms = B.autotune(cache)
-    out = torch.empty((rays, 4), dtype=torch.float32, device="cuda")
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    stream = torch.cuda.Stream()
-    for _ in range(args.warmup):
-        B.render_device(out, stream)
-    torch.cuda.synchronize()
-    ts = []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            B.render_device(out, stream)
-            e1.record(stream)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
         torch.cuda.synchronize()
-        ts.append(e0.elapsed_time(e1))
-    ms = float(np.mean(ts))
-    st = B.stats()
-    # the same 64 cameras as 64 separate launches (one context each)
-    ctxs = [G.Renderer(c) for c in cams]
-    for R in ctxs:
-        R.set_precision(form)
-    bufs = [torch.empty((c["height"], c["width"], 4), dtype=torch.float32, device="cuda") for c in cams]
-    for _ in range(max(1, args.warmup)):
-        for R, b in zip(ctxs, bufs):
-            R.render_device(b, None, None, stream)
-    torch.cuda.synchronize()
-    sep = []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for R, b in zip(ctxs, bufs):
-                R.render_device(b, None, None, stream)
-            e1.record(stream)
-        torch.cuda.synchronize()
-        sep.append(e0.elapsed_time(e1))
-    sep_ms = float(np.mean(sep))
-    mixed_vs_fp64 = None
-    if form == G.FORM_MIXED:
-        # the same batch in the FP64 form: time, and the mixed images' error
-        got = out.cpu().numpy()
-        B64 = G.Batch(cams)
-        B64.autotune(cache)
-        out64 = torch.empty_like(out)
-        for _ in range(max(1, args.warmup)):
-            B64.render_device(out64, stream)
-        torch.cuda.synchronize()
-        t64 = []
+        ts = []
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                B64.render_device(out64, stream)
+                fn()
                 e1.record(stream)
             torch.cuda.synchronize()
-            t64.append(e0.elapsed_time(e1))
+            ts.append(e0.elapsed_time(e1))
+        return float(np.mean(ts))
+
+    B = G.Batch(cams)
+    B.set_precision(form)
+    tuned_ms = B.autotune(cache)
+    out = torch.empty((rays, 4), dtype=torch.float32, device="cuda")
+    ms = timed(lambda: B.render_device(out, stream))
+    st = B.stats()
+    got = out.cpu().numpy()
+    # the same 64 cameras as 64 separate launches (one context each)
+    ctxs = [G.Renderer(c) for c in cams]
+    for R in ctxs:
+        R.set_precision(form)
+    bufs = [torch.empty((c["height"], c["width"], 4), dtype=torch.float32, device="cuda") for c in cams]
+
+    def separate():
+        for R, bb in zip(ctxs, bufs):
+            R.render_device(bb, None, None, stream)
+    sep_ms = timed(separate)
+    for R in ctxs:
+        R.close()
+    res = {"metric": "batched sweep rays/s (64 Kerr cameras x 256^2, one persistent launch)",
+           "value": rays / (ms * 1e-3), "unit": "rays/s", "ms_per_step": ms, "form": form_name,
+           "dtype": "f64" if form == G.FORM_FP64 else "f32+f64",
+           "config": {"workload": "sweep_64cams_spins0_0.5_0.9_0.998_x16incl_5to90deg_256x256_thin_disk_stars",
+                      "rays_per_step": rays, "l2": "flushed between steps (256 MiB write)"},
+           "schedule": dict(zip(("chunk", "order", "blocks_per_sm"), B.schedule()), autotune_ms=tuned_ms,
+                            **B.tuning()),
+           "separate_launches_ms_per_step": sep_ms, "batched_speedup": sep_ms / ms,
+           "work": {"attempts_per_ray": st["attempts"] / max(1, st["rays"]),
+                    "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])},
+           # FP64: one persistent launch; mixed: speculate, stars, re-trace, resolve
+           "gpu_launches_per_step": 4 if form == G.FORM_MIXED else 1}
+    if form == G.FORM_MIXED:
+        B64 = G.Batch(cams)
+        t64 = B64.autotune(cache)
+        out64 = torch.empty_like(out)
+        ms64 = timed(lambda: B64.render_device(out64, stream))
         ref = out64.cpu().numpy()
-        scale = float(ref[:, :3].max())
-        rel = np.abs(got[:, :3] - ref[:, :3]) / np.maximum(np.abs(ref[:, :3]), 1e-6 * scale)
-        mixed_vs_fp64 = {"fp64_batch_ms": float(np.mean(t64)), "speedup": float(np.mean(t64)) / ms,
-                         "max_rel_err": float(rel.max()), "pixels_above_1e-4": int(np.sum(rel.max(axis=1) > 1e-4)),
-                         "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])}
+        worst, over = 0.0, 0
+        for k in range(len(cams)):
+            a, b = int(B.offsets[k]), int(B.offsets[k + 1])
+            r, g = ref[a:b, :3], got[a:b, :3]
+            scale = float(r.max())
+            rel = np.abs(g - r) / np.maximum(np.abs(r), 1e-6 * scale)
+            worst = max(worst, float(rel.max()))
+            over += int(np.sum(rel.max(axis=1) > 1e-4))
+        res["fp64_batch"] = {"ms_per_step": ms64, "value": rays / (ms64 * 1e-3), "autotune_ms": t64,
+                             "schedule": dict(zip(("chunk", "order", "blocks_per_sm"), B64.schedule()),
+                                              **B64.tuning())}
+        res["speedup_mixed_vs_fp64_batch"] = ms64 / ms
+        res["mixed_error_vs_fp64"] = {"max_rel": worst, "pixels_above_1e-4": over,
+                                      "rel_floor": "max(|fp64|, 1e-6 x camera max)"}
         B64.close()
-    chunk, order, bps = B.schedule()
-    line = {"metric": "batched sweep rays/s (64 Kerr cameras x 256^2, one persistent launch)", "value": rays / (ms * 1e-3),
-            "unit": "rays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "dtype": "f64" if form == G.FORM_FP64 else "f32+f64", "data": "synthetic",
-            "config": {"workload": "sweep_64cams_spins0_0.5_0.9_0.998_x16incl_5to90deg_256x256_thin_disk_stars",
-                       "rays_per_step": rays, "schedule": {"chunk": chunk, "order": ["camera-major", "round-robin"][order],
-                                                           "blocks_per_sm": bps, "autotune_ms": tuned_ms},
-                       "l2": "flushed between steps"},
-            "separate_launches_ms_per_step": sep_ms, "batched_speedup": sep_ms / ms,
-            "work": {"attempts_per_ray": st["attempts"] / max(1, st["rays"])},
-            # FP64: one persistent launch; mixed: speculate, stars, re-trace, resolve
-            "gpu_launches": args.steps * (4 if form == G.FORM_MIXED else 1)}
-    if mixed_vs_fp64 is not None:
-        line["mixed_vs_fp64_batch"] = mixed_vs_fp64
-    print(json.dumps(line), flush=True)
+    B.close()
+    return res
+
+
+def run_batch(args):
+    import torch
+    import grrt_b200 as G
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res = batch_section(args, torch, G, stream, flush, args.form)
+    res.update(n_gpus=1, steps=args.steps, warmup=args.warmup, higher_is_better=True, data="synthetic",
+               gpu_launches=args.steps * res["gpu_launches_per_step"])
+    print(json.dumps(res), flush=True)
 
 
 def time_form(torch, R, form, stream, flush, render, steps, warmup, dist):
@@ -680,8 +684,9 @@ def main():
         res["clocks"] = clocks.stop()
         res.update(n_gpus=1, steps=args.steps, warmup=args.warmup, unit="pixel*frequency/s",
                    higher_is_better=True, data="synthetic", dtype="f32+f64",
-                   # mixed form per frame: speculation, the list ordering's four kernels, re-trace, resolve
-                   gpu_launches=args.steps * 7)
+                   # mixed form per frame: speculation, the longest-first ordering's three kernels,
+                   # re-trace, resolve
+                   gpu_launches=args.steps * 6)
         print(json.dumps(res), flush=True)
         return
     if (args.width, args.height) != (W, H):
@@ -864,6 +869,11 @@ def main():
                 line["surrogate"] = run_surrogate(args, torch, G, stream, flush, peaks)
             except Exception as ex:  # reported, the headline stands on its own
                 line["surrogate"] = {"error": str(ex)}
+        if not args.no_batch_section and world == 1:
+            try:
+                line["batch"] = batch_section(args, torch, G, stream, flush, "mixed")
+            except Exception as ex:  # reported, the headline stands on its own
+                line["batch"] = {"error": str(ex)}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -46,7 +46,24 @@ struct LaunchResources {
     const volatile int* cancel = nullptr;  // host-mapped cancel flag, may be null
     double* spectral_scratch = nullptr;    // spectral transfer state, see volume_spectral_scratch_elems
     size_t spectral_scratch_elems = 0;
+    // volumetric FP64 forms: the longest-first pixel order (order_by_cost)
+    // and its scratch, volume_order_bytes(tile); NULL: pixels in index order
+    void* order_scratch = nullptr;
+    size_t order_scratch_bytes = 0;
 };
+
+// Bytes of LaunchResources::order_scratch a volumetric launch over `tile` uses.
+size_t volume_order_bytes(const DevTile& tile);
+
+// Longest-first order of n work items (cost_order.cu): items (NULL: 0..n-1;
+// the count may be on the device, n_dev, at most n) are pixels of the tile
+// (is_sample false: keyed by each pixel's first sample) or samples
+// pixel * grid^2 + s; out receives them ordered by the closed-form distance of
+// their camera ray to the critical curve, nearest first. scratch:
+// cost_order_scratch_bytes(n).
+size_t cost_order_scratch_bytes(size_t n);
+cudaError_t order_by_cost(const DevScene& S, const DevTile& tile, const unsigned* items, unsigned n,
+                          const unsigned* n_dev, bool is_sample, unsigned* out, void* scratch, cudaStream_t stream);
 
 // Doubles of spectral scratch a launch with nb bins needs on the current device.
 size_t volume_spectral_scratch_elems(int nb);
