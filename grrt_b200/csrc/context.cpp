@@ -360,6 +360,7 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     progress_total = (mixed_thin || mixed_vol) ? static_cast<unsigned>(tile.w) * tile.h * (S.grid * S.grid)
                                                : static_cast<unsigned>(tile.w) * tile.h;
     progress_header = (mixed_thin || mixed_vol) ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
+    progress_done = vol != nullptr;
     cudaEventRecord(ev0, s);
     cudaError_t e;
     if (mixed_vol)
@@ -392,11 +393,15 @@ int GRRTContext::wait_with_progress(cudaStream_t s, grrt_progress_fn cb, void* u
             while (cudaStreamQuery(s) == cudaErrorNotReady) {
                 std::this_thread::sleep_for(std::chrono::milliseconds(5));
                 h_q[0] = h_q[1] = h_q[2] = 0;
-                if (cudaMemcpyAsync(h_q, d_queue, sizeof(unsigned), cudaMemcpyDeviceToHost, poll) != cudaSuccess)
+                // single pass: items finished (volumetric) or taken; mixed
+                // forms: speculation items taken, then re-trace items
+                const bool single_done = progress_done && !progress_header;
+                if (cudaMemcpyAsync(h_q, d_queue + (single_done ? 1 : 0), sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                    poll) != cudaSuccess)
                     break;
                 if (progress_header &&
-                    (cudaMemcpyAsync(h_q + 1, progress_header + 256, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                                     poll) != cudaSuccess ||
+                    (cudaMemcpyAsync(h_q + 1, progress_header + (progress_done ? 260 : 256), sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost, poll) != cudaSuccess ||
                      cudaMemcpyAsync(h_q + 2, progress_header + 512, sizeof(unsigned), cudaMemcpyDeviceToHost,
                                      poll) != cudaSuccess))
                     break;
@@ -596,6 +601,7 @@ int GRRTContext::render_spectral_tile(const DevTile& tile, double* d_spec, unsig
     progress_total = mixed ? static_cast<unsigned>(width) * height * (S.grid * S.grid)
                            : static_cast<unsigned>(width) * height;
     progress_header = mixed ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
+    progress_done = true;
     cudaEventRecord(ev0, s);
     const cudaError_t e =
         mixed ? launch_volume_spectral_mixed(S, tile, d_freqs, nb, out, res, d_mixed_scratch, d_mixed_scratch_bytes,

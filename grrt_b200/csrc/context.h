@@ -49,6 +49,10 @@ struct GRRTContext {
     // scratch header with the re-trace counter (+256) and list length (+512)
     unsigned progress_total = 0;
     const unsigned char* progress_header = nullptr;
+    // volumetric kernels also count finished items (d_queue[1], header + 260),
+    // which progress reads instead of the items taken (their long rays finish
+    // long after the last item is taken)
+    bool progress_done = false;
 
     // Device state (created at the first render).
     int device = -1;

@@ -421,7 +421,9 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
         }
         if (live && term >= 0) {
             live = false;
-            h_max = fmaxf(h_max, static_cast<float>(fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt)));
+            if (term != kTermHorizon)  // as the FP64 form: rays that do not end at the horizon
+                h_max = fmaxf(h_max,
+                              static_cast<float>(fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt)));
             if (term == kTermEscaped && S.stars_on) {
                 const double b = star_brightness(S.stars, y.th, y.ph);
                 c0 += b;

@@ -237,7 +237,10 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
         // ---- finish a terminated sample ----
         if (live && term >= 0) {
             live = false;
-            cold.h_max = fmax(cold.h_max, fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt));
+            // the constraint at the final state of rays that do not end at the
+            // horizon (there Delta -> 0 and P^2 / Delta cancels catastrophically)
+            if (term != kTermHorizon)
+                cold.h_max = fmax(cold.h_max, fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt));
             double c0 = cold.col[0], c1 = cold.col[1], c2 = cold.col[2];
             if (term == kTermEscaped) {
                 ++cold.escaped;

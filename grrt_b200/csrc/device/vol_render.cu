@@ -203,6 +203,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
                 const unsigned ne = (entries > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(entries);
                 out_fate[q] = static_cast<unsigned>(term) | (ne << 2);
                 pix = -1;
+                atomicAdd(queue + 1, 1u);  // finished items, for progress reports
             } else {
                 for (int ch = 0; ch < 3; ++ch) acc[ch] = acc[ch] + col[ch];
                 if (out_fate) {
@@ -222,6 +223,7 @@ vol_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4
                         out_d[3 * o + 2] = r2;
                     }
                     pix = -1;
+                    atomicAdd(queue + 1, 1u);  // finished items, for progress reports
                 }
             }
         }
@@ -268,7 +270,7 @@ cudaError_t launch_volume_rgb(const DevScene& S, const DevTile& tile, const Thin
     int blocks = sms * per;
     const int needed = static_cast<int>((total + kVolThreads - 1) / kVolThreads);
     if (needed < blocks) blocks = needed;
-    cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
+    cudaError_t e = cudaMemsetAsync(res.queue, 0, 2 * sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
     vol_render_kernel<false><<<blocks, kVolThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
                                                                  res.stats, res.cancel, nullptr, nullptr);

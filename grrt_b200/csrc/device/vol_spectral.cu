@@ -402,6 +402,9 @@ vol_spectral_kernel(const __grid_constant__ DevScene S0, const DevTile tile, con
             // I nu^3 of the finished samples into the pixel sums; finished pixels stored
             const unsigned fm = __ballot_sync(kWarp, finish);
             const unsigned dm = __ballot_sync(kWarp, pixel_done);
+            // finished work items, for progress reports (the work counter
+            // counts items taken; the long rays finish long after)
+            if (dm && lane == 0) atomicAdd(queue + 1, static_cast<unsigned>(__popc(dm)));
             for (unsigned m = fm; m; m &= m - 1) {
                 const int src = __ffs(m) - 1;
                 const size_t o = __shfl_sync(kWarp, static_cast<unsigned long long>(out_elem), src);
@@ -712,7 +715,8 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
     if (needed < blocks) blocks = needed;
     if (!res.spectral_scratch || res.spectral_scratch_elems < static_cast<size_t>(4) * nb * blocks * kSpecThreads)
         return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
+    // work counter and finished-items counter
+    cudaError_t e = cudaMemsetAsync(res.queue, 0, 2 * sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
     // longest rays first
     unsigned* order = nullptr;
@@ -750,7 +754,7 @@ cudaError_t launch_vol_spectral_batch(const DevBatch& B, int nb_max, double* out
     if (B.n_chunks <= 0) return cudaSuccess;
     if (nb_max < 1 || !scratch || scratch_elems < static_cast<size_t>(4) * nb_max * blocks * kSpecThreads)
         return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned), stream);
+    cudaError_t e = cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
     vol_spectral_kernel<false, true><<<blocks, kSpecThreads, 0, stream>>>(
         DevScene{}, DevTile{}, nullptr, nb_max, out_spec, nullptr, scratch, queue, stats, nullptr, nullptr, nullptr, B);

@@ -48,9 +48,10 @@ typedef struct {
     unsigned long long fp64_attempts; /* attempts evaluated in FP64 */
     double kernel_ms;                 /* device time of the render kernels (CUDA events) */
     double hamiltonian_max;           /* thin-disk FP64 traces (FP64 form, the mixed form's
-                                         re-trace): max over samples of |H| / p_t^2 at the final
-                                         state, H = 1/2 g^{mu nu} p_mu p_nu (0 on the light cone);
-                                         0 where not measured */
+                                         re-trace): max over the samples that do not end at the
+                                         horizon of |H| / p_t^2 at the final state,
+                                         H = 1/2 g^{mu nu} p_mu p_nu (0 on the light cone; near the
+                                         horizon its evaluation cancels); 0 where not measured */
 } GRRTStats;
 
 /* Select the precision form for later renders (src/geodesic_tracer.cpp:100 is

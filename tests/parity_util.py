@@ -2,6 +2,12 @@
 the C ABI, run the same samples through the oracle, and derive the
 rounding-sensitive ("caustic") band from the oracle itself.
 
+Image-integrated flux. The volumetric march amplifies rounding: the probes
+move a volumetric frame's flux per bin by ~1e-3 relative (the reference's own
+strict and as-shipped builds differ per pixel by a median of ~5%), so the
+flux bar of a device render is data-driven: within twice the largest move of
+any probe (OracleRGB / OracleSpectral.probe_flux_spread).
+
 Band definition. A sample is rounding-sensitive when the strict oracle and a
 rounding-level probe disagree on the fate or differ by more than the test
 tolerance. The probes are the same oracle compiled with FMA contraction and
@@ -61,6 +67,14 @@ def hull_error(got: np.ndarray, lo: np.ndarray, hi: np.ndarray, floor: float = 1
     return np.max(np.maximum(out, 0.0) / scale, axis=1)
 
 
+def flux_spread(a: np.ndarray, b: np.ndarray) -> float:
+    """Largest relative difference over channels (or bins) of the image-
+    integrated flux of two sets of pixels."""
+    fa, fb = a.sum(axis=0), b.sum(axis=0)
+    floor = 1e-300 + 1e-12 * float(np.max(np.abs(fb))) if fb.size else 1e-300
+    return float(np.max(np.abs(fa - fb) / np.maximum(np.abs(fb), floor))) if fb.size else 0.0
+
+
 def pixel_mean(per_sample: np.ndarray, spp: int) -> np.ndarray:
     """The reference's spp mean: accumulate samples in order from 0, then scale."""
     grid = max(1, int(math.sqrt(spp)))
@@ -84,6 +98,7 @@ class OracleRGB:
         px, py = oracle_bind.jittered_samples(W, H, spp, pix)
         O = oracle_bind.Oracle(R)
         self.rgb, self.term, self.ncross, self.fin, self.counters = O.trace_rgb(px, py)
+        spreads = []
         self.sensitive = np.zeros(len(px), dtype=bool)
         self.fate_sensitive = np.zeros(len(px), dtype=bool)
         lo, hi = self.rgb.copy(), self.rgb.copy()
@@ -98,7 +113,10 @@ class OracleRGB:
                 self.sensitive |= fs
                 self.sensitive |= np.any(np.abs(r2 - self.rgb) > tol * np.abs(self.rgb), axis=1)
                 lo, hi = np.minimum(lo, r2), np.maximum(hi, r2)
+                spreads.append(flux_spread(pixel_mean(r2, spp), pixel_mean(self.rgb, spp)))
         self.pixel_rgb = pixel_mean(self.rgb, spp)
+        # how far rounding-level probes move the image-integrated flux (per channel, relative)
+        self.probe_flux_spread = max(spreads) if spreads else 0.0
         # per pixel, the range the oracle and its rounding probes span
         self.pixel_lo, self.pixel_hi = pixel_mean(lo, spp), pixel_mean(hi, spp)
         self.pixel_band = self.sensitive.reshape(-1, self.g2).any(axis=1)
@@ -114,6 +132,7 @@ class OracleSpectral:
         px, py = oracle_bind.jittered_samples(W, H, spp, pix)
         O = oracle_bind.Oracle(R)
         self.spec, self.term, self.counters = O.trace_spectral(freqs, px, py)
+        spreads = []
         self.sensitive = np.zeros(len(px), dtype=bool)
         self.fate_sensitive = np.zeros(len(px), dtype=bool)
         lo, hi = self.spec.copy(), self.spec.copy()
@@ -127,7 +146,10 @@ class OracleSpectral:
                 self.sensitive |= t2 != self.term
                 self.sensitive |= np.any(np.abs(s2 - self.spec) > tol * np.abs(self.spec), axis=1)
                 lo, hi = np.minimum(lo, s2), np.maximum(hi, s2)
+                spreads.append(flux_spread(pixel_mean(s2, spp), pixel_mean(self.spec, spp)))
         self.pixel_spec = pixel_mean(self.spec, spp)
+        # how far rounding-level probes move the image-integrated flux (per bin, relative)
+        self.probe_flux_spread = max(spreads) if spreads else 0.0
         self.pixel_lo, self.pixel_hi = pixel_mean(lo, spp), pixel_mean(hi, spp)
         self.pixel_band = self.sensitive.reshape(-1, self.g2).any(axis=1)
         self.pixel_fate_band = self.fate_sensitive.reshape(-1, self.g2).any(axis=1)

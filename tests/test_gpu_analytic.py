@@ -36,7 +36,7 @@ def test_schwarzschild_shadow_edge(grrt, need_gpu):
     psi_c = math.asin(3.0 * math.sqrt(3.0) * M / r_obs * math.sqrt(1.0 - 2.0 * M / r_obs))
     pix = fov / W  # one pixel, in radians
     inside, outside = psi[term == 0], psi[term == 1]
-    assert len(inside) > 3000 and len(outside) > 3000
+    assert len(inside) > 500 and len(outside) > 3000  # the shadow covers ~pi * 17^2 pixels
     assert np.count_nonzero(term == 2) < 10, "rays near the photon sphere hit the step budget"
     edge_in, edge_out = inside.max(), outside.min()
     edge = 0.5 * (edge_in + edge_out)
@@ -66,12 +66,15 @@ def hamiltonian_np(M, a, fin):
 
 
 def test_hamiltonian_constraint(grrt, need_gpu):
-    """|H| / p_t^2 at every sample's final state stays near 0 (README.md:213;
-    the reference's CUDA tests hold |H| < 1e-7 along a geodesic,
-    cuda/tests/test_cuda.cu:385-402). The device reports the maximum over the
-    frame (GRRTStats.hamiltonian_max); the oracle's final states of the same
-    samples give the same order of magnitude. Camera rays start null to 1e-10
-    (the reference's camera test)."""
+    """|H| / p_t^2 at the final state of every sample that does not end at
+    the horizon stays below 1e-7 (README.md:213; the reference's CUDA tests
+    hold |H| < 1e-7 along a geodesic, cuda/tests/test_cuda.cu:385-402). The
+    device reports the maximum over the frame (GRRTStats.hamiltonian_max); the
+    oracle's final states of the same samples give the same value. At the
+    horizon stop (r_h + 0.01) Delta -> 0 and the P^2 / Delta term cancels, so
+    the evaluation itself loses digits there (measured up to ~5e-4) and those
+    samples are left out. Camera rays start null to 1e-10 (the reference's
+    camera test)."""
     import torch
     from parity_util import OracleRGB
 
@@ -83,11 +86,11 @@ def test_hamiltonian_constraint(grrt, need_gpu):
     h_dev = R.stats()["hamiltonian_max"]
     orc = OracleRGB(R, np.arange(W * H), 1e-9, band=False)
     M, a = R.table("scalars")[:2]
-    h_orc = np.abs(hamiltonian_np(M, a, orc.fin)) / orc.fin[:, 4] ** 2
-    print(f"\n  max |H|/p_t^2 at the final states: device {h_dev:.3e}, oracle {h_orc.max():.3e} "
-          f"(oracle median {np.median(h_orc):.3e})")
+    h_orc = (np.abs(hamiltonian_np(M, a, orc.fin)) / orc.fin[:, 4] ** 2)[orc.term != 0]
+    print(f"\n  max |H|/p_t^2 at the final states (not at the horizon): device {h_dev:.3e}, oracle "
+          f"{h_orc.max():.3e} (oracle median {np.median(h_orc):.3e})")
     assert 0.0 < h_dev < 1e-7
-    assert h_dev < 100.0 * h_orc.max() + 1e-12 and h_orc.max() < 100.0 * h_dev + 1e-12
+    assert 0.5 * h_orc.max() <= h_dev <= 2.0 * h_orc.max()
     # camera rays are null
     px, py = oracle_bind.jittered_samples(W, H, 1, np.arange(0, W * H, 97))
     cam = np.array([R.camera_ray(x, y) for x, y in zip(px, py)])

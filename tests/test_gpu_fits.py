@@ -14,8 +14,9 @@ and odd image sizes; 1 and 4 spp):
     oracle's probes, tests/parity_util.py) at least 99% of the pixels are
     within 1e-9 relative and every one within 1e-6; every pixel lies within
     1e-6 of the range that the oracle and its rounding probes span, or the
-    band holds it (counted and bounded); the image-integrated flux per bin is
-    within 1e-6 relative.
+    band holds it; the image-integrated flux per bin is within twice the move
+    that the rounding-level probes themselves make in it (the volumetric march
+    amplifies rounding: the probes move it by ~1e-3).
 """
 import json
 import os
@@ -23,7 +24,7 @@ import os
 import numpy as np
 import pytest
 
-from parity_util import OracleSpectral, hull_error, rel_err
+from parity_util import OracleSpectral, flux_spread, hull_error, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -83,15 +84,16 @@ def test_fits_file_matches_reference(grrt, need_gpu, golden, tmp_path, case):
     within = float(np.mean(err[out] <= TOL)) if out.any() else 1.0
     worst = float(np.max(err[out])) if out.any() else 0.0
     herr = hull_error(got, orc.pixel_lo, orc.pixel_hi)
-    flux_g, flux_w = got.sum(axis=0), want.sum(axis=0)
-    ferr = float(np.max(rel_err(flux_g, flux_w, floor=1e-300 + 1e-12 * np.max(np.abs(flux_w)))))
+    ferr = flux_spread(got, want)
+    fbar = max(1e-9, 2.0 * orc.probe_flux_spread)
     print(f"\n  [{case}] band {orc.pixel_band.mean():.4f}; outside band within {TOL}: {within:.5f}, worst "
           f"{worst:.2e}; outside the probe range by > {LOOSE}: {int(np.sum(herr > LOOSE))} pixels "
-          f"(max {herr.max():.2e}); integrated flux per bin: max rel err {ferr:.2e}")
+          f"(max {herr.max():.2e}); integrated flux per bin: max rel err {ferr:.2e} (probes move it by "
+          f"{orc.probe_flux_spread:.2e})")
     assert within >= 0.99
     assert worst <= LOOSE
     assert np.all((herr <= LOOSE) | orc.pixel_band)
-    assert ferr <= LOOSE
+    assert ferr <= fbar
 
 
 def test_fits_repeated_and_larger_than_one_copy_group(grrt, need_gpu, tmp_path):

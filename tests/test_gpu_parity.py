@@ -16,7 +16,8 @@ import math
 import numpy as np
 import pytest
 
-from parity_util import OracleRGB, OracleSpectral, device_render_rgb, device_render_spectral, hull_error, rel_err
+from parity_util import (OracleRGB, OracleSpectral, device_render_rgb, device_render_spectral, flux_spread, hull_error,
+                         rel_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -24,10 +25,13 @@ TOL = 1e-9
 LOOSE = 1e-6
 MIN_WITHIN = 0.99
 MAX_BAND = 0.06  # fraction of pixels allowed in the rounding-sensitive band (1 spp)
-# image-integrated flux per frequency bin (band pixels included)
-FLUX_TOL = 1e-6
-# fraction of band pixels allowed outside the oracle's probe range by more than LOOSE
-MAX_BAND_OFF = 0.25
+# image-integrated flux per channel or bin (band pixels included): within
+# FLUX_PROBES x the largest move of a rounding-level probe, and at least 1e-9
+FLUX_PROBES = 2.0
+# thin disk: fraction of band pixels allowed outside the oracle's probe range
+# by more than LOOSE (measured: at most 2.3%); volumetric band pixels are
+# chaotic (the march amplifies rounding), so there the flux bar holds them
+MAX_BAND_OFF = 0.05
 
 
 def report(R, frac, within, err, out, stats, ocnt):
@@ -39,23 +43,31 @@ def report(R, frac, within, err, out, stats, ocnt):
           f"{ocnt['attempts']}")
 
 
-def check_band(got, orc, band):
+def check_band(got, orc, band, volumetric=False):
     """Band pixels: each must lie within LOOSE of the range spanned by the
     oracle and its rounding probes (a pixel whose samples the probes send to
     different fates can land anywhere in between, or, on a chaotic
-    near-critical orbit, outside it: those are counted and bounded)."""
+    near-critical orbit, outside it: those are counted and bounded). The
+    image-integrated flux, band pixels included, stays within FLUX_PROBES x
+    the probes' own move of it."""
     herr = hull_error(got, orc.pixel_lo, orc.pixel_hi)
     assert np.all(herr[~band] <= LOOSE + 1e-9)  # outside the band the hull holds the 1e-6 bar above
     n_band = int(band.sum())
     off = int(np.sum(herr[band] > LOOSE))
+    want = orc.pixel_rgb if hasattr(orc, "pixel_rgb") else orc.pixel_spec
+    ferr = flux_spread(got, want)
+    fbar = max(1e-9, FLUX_PROBES * orc.probe_flux_spread)
     print(f"  band pixels: {n_band}; outside the probe range by more than {LOOSE}: {off}"
-          + (f" (max {herr[band].max():.2e})" if n_band else ""))
-    assert off <= max(2, int(MAX_BAND_OFF * n_band)), f"{off} of {n_band} band pixels outside the probe range"
+          + (f" (max {herr[band].max():.2e})" if n_band else "")
+          + f"; integrated flux: rel err {ferr:.2e}, probes move it by {orc.probe_flux_spread:.2e}")
+    if not volumetric:
+        assert off <= max(2, int(MAX_BAND_OFF * n_band)), f"{off} of {n_band} band pixels outside the probe range"
+    assert ferr <= fbar, f"integrated flux differs by {ferr:.3e} (bar {fbar:.3e})"
     return off
 
 
 def check_rgb(grrt, R, pix_all: bool = True, n_sample: int = 0, seed: int = 0, max_band=MAX_BAND,
-              same_work: bool = True):
+              same_work: bool = True, volumetric: bool = False):
     W, H = R.width, R.height
     spp = R.values.get("samples_per_pixel", 1)
     rgba, rgb64, fate, stats = device_render_rgb(R, spp)
@@ -87,7 +99,7 @@ def check_rgb(grrt, R, pix_all: bool = True, n_sample: int = 0, seed: int = 0, m
     report(R, frac, within, err, out, stats, orc.counters)
     assert within >= MIN_WITHIN, f"only {within:.4%} of pixels outside the band within {TOL}"
     assert worst <= LOOSE, f"max relative error outside the band {worst:.3e}"
-    check_band(got, orc, band)
+    check_band(got, orc, band, volumetric)
     # work: same method, so the attempt count matches the oracle's closely
     if pix_all and same_work:
         assert abs(stats["attempts"] - orc.counters["attempts"]) <= 0.01 * orc.counters["attempts"]
@@ -104,7 +116,7 @@ def test_schwarzschild_thin_256_full_image(grrt, need_gpu):
 
 def test_kerr_thin_stars_4spp(grrt, need_gpu):
     R = grrt.Renderer(grrt.config_params(2, width=160, height=160))  # 4 spp, stars
-    frac, worst, stats, orc = check_rgb(grrt, R, max_band=0.15)
+    frac, worst, stats, orc = check_rgb(grrt, R, max_band=0.08)  # measured 0.058
     assert (orc.ncross > 1).any(), "higher-order images expected"
     print(f"\nC2 160^2x4: band {frac:.4%}, worst {worst:.2e}")
 
@@ -112,7 +124,7 @@ def test_kerr_thin_stars_4spp(grrt, need_gpu):
 def test_kerr_thin_full_size_sampled(grrt, need_gpu):
     """The 1024^2 4-spp scene at full size; parity on a random pixel subset."""
     R = grrt.Renderer(grrt.config_params(2))
-    frac, worst, stats, orc = check_rgb(grrt, R, pix_all=False, n_sample=1500, seed=5, max_band=0.15)
+    frac, worst, stats, orc = check_rgb(grrt, R, pix_all=False, n_sample=1500, seed=5, max_band=0.08)  # 0.055
     assert stats["rays"] == 1024 * 1024 * 4
     print(f"\nC2 1024^2x4 sampled: band {frac:.4%}, worst {worst:.2e}, attempts/ray "
           f"{stats['attempts'] / stats['rays']:.1f}")
@@ -120,11 +132,12 @@ def test_kerr_thin_full_size_sampled(grrt, need_gpu):
 
 # (scene overrides, band allowance): a pixel joins the band when any of its
 # samples is rounding-sensitive, so the allowance grows with spp and with the
-# share of the frame the disk covers.
+# share of the frame the disk covers. Allowances: the measured band on B200
+# (0.201, 0.042, 0.486) plus a margin.
 @pytest.mark.parametrize("variant,max_band", [
-    (dict(spin=0.5, observer_theta=math.radians(30.0)), 0.3),
-    (dict(spin=0.9, observer_theta=math.radians(89.0), observer_phi=1.0, disk_inner=8.0, disk_outer=30.0), 0.3),
-    (dict(metric_type=0, observer_r=20.0, fov=math.radians(40.0), samples_per_pixel=9), 0.7),
+    (dict(spin=0.5, observer_theta=math.radians(30.0)), 0.25),
+    (dict(spin=0.9, observer_theta=math.radians(89.0), observer_phi=1.0, disk_inner=8.0, disk_outer=30.0), 0.08),
+    (dict(metric_type=0, observer_r=20.0, fov=math.radians(40.0), samples_per_pixel=9), 0.55),
 ])
 def test_thin_variants(grrt, need_gpu, variant, max_band):
     vals = grrt.config_params(2, width=64, height=48, **variant)
@@ -135,7 +148,7 @@ def test_thin_variants(grrt, need_gpu, variant, max_band):
 def test_volumetric_rgb(grrt, need_gpu):
     freqs = grrt.log_bins(1e14, 1e18, 32)
     R = grrt.Renderer(grrt.config_params(3, width=64, height=64), freqs=freqs)
-    frac, worst, stats, orc = check_rgb(grrt, R, max_band=0.3)
+    frac, worst, stats, orc = check_rgb(grrt, R, max_band=0.1, volumetric=True)  # measured 0.072
     assert stats["march_steps"] > 0 and stats["physics_steps"] > 0
     assert stats["march_steps"] == orc.counters["march_steps"] or frac > 0
     print(f"\nC3 RGB 64^2: band {frac:.4%}, worst {worst:.2e}")
@@ -161,12 +174,7 @@ def check_spectral(grrt, R, freqs, pix, max_band):
     report(R, frac, within, err, out, stats, orc.counters)
     assert within >= MIN_WITHIN, f"only {within:.4%} of pixels outside the band within {TOL}"
     assert worst <= LOOSE, f"max relative error outside the band {worst:.3e}"
-    check_band(got, orc, band)
-    # image-integrated flux per bin over every checked pixel, band included
-    fg, fo = got.sum(axis=0), orc.pixel_spec.sum(axis=0)
-    ferr = float(np.max(rel_err(fg, fo, floor=1e-300 + 1e-12 * np.max(np.abs(fo)))))
-    print(f"  integrated flux per bin: max relative error {ferr:.2e}")
-    assert ferr <= FLUX_TOL, f"integrated flux per bin differs by {ferr:.3e}"
+    check_band(got, orc, band, volumetric=True)
     assert stats["bin_updates"] == stats["physics_steps"] * nb
     return frac, worst, stats
 
@@ -174,7 +182,7 @@ def check_spectral(grrt, R, freqs, pix, max_band):
 def test_volumetric_spectral(grrt, need_gpu):
     freqs = grrt.log_bins(1e14, 1e18, 32)
     R = grrt.Renderer(grrt.config_params(3, width=64, height=64), freqs=freqs)
-    frac, worst, stats = check_spectral(grrt, R, freqs, np.arange(64 * 64), max_band=0.3)
+    frac, worst, stats = check_spectral(grrt, R, freqs, np.arange(64 * 64), max_band=0.1)  # measured 0.072
     print(f"\nC3 spectral 64^2x32: band {frac:.4%}, worst {worst:.2e}, physics steps {stats['physics_steps']}")
 
 
@@ -182,7 +190,7 @@ def test_volumetric_spectral_full_size_sampled(grrt, need_gpu):
     freqs = grrt.log_bins(1e14, 1e18, 32)
     R = grrt.Renderer(grrt.config_params(3), freqs=freqs)  # 512^2
     pix = np.random.default_rng(9).choice(512 * 512, size=600, replace=False)
-    frac, worst, stats = check_spectral(grrt, R, freqs, pix, max_band=0.3)
+    frac, worst, stats = check_spectral(grrt, R, freqs, pix, max_band=0.1)  # measured 0.068
     assert stats["rays"] == 512 * 512
 
 
