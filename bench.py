@@ -604,20 +604,26 @@ def run_surrogate(args, torch, G, stream, flush, peaks):
     rel = (np.abs(a - b) / np.maximum(np.abs(b), 1e-6 * scale)).max(axis=2)
     lit = b.max(axis=2) > 1e-6 * scale
     fates_fp64 = rfate.cpu().numpy()
-    # Speed against colour error: the colour tolerance tol_rel sets which lit
-    # samples the network shades (those whose calibrated crossing band moves
-    # the colour by at most tol_rel); the rest are re-traced in FP64. Errors
-    # are against the FP64 form, on lit pixels (colour above 1e-6 x the frame
-    # maximum), so they are the network's own errors on the samples it shades.
+    # Speed against colour error. Which samples the network decides is set by
+    # the calibrated bands (the u error band in multiples of each sample's
+    # predicted sigma, the critical-curve and graze bands around the
+    # closed-form classification) and the colour tolerance tol_rel (a lit
+    # sample is shaded by the network when its crossing band moves the colour
+    # by at most tol_rel); the rest are re-traced in FP64. The sweep narrows
+    # the bands by a factor and widens tol_rel. Errors are against the FP64
+    # form, on lit pixels (colour above 1e-6 x the frame maximum), so they are
+    # the network's own errors on the samples it decides.
     bands0 = S.bands()
     pareto = []
-    for tol in (1e-3, 3e-3, 1e-2, 3e-2, 1e-1):
-        S.set_bands(bands0["du"], bands0["dir"], bands0["capture"], bands0["graze"], tol)
+    for shrink, tol in ((1.0, 1e-3), (1.0, 1e-2), (0.5, 1e-3), (0.5, 1e-2), (0.25, 1e-2), (0.1, 1e-2),
+                        (0.1, 1e-1)):
+        S.set_bands(bands0["du"] * shrink, bands0["dir"] * shrink, bands0["capture"] * shrink,
+                    bands0["graze"] * shrink, tol)
         ms_t = timed(lambda: S.render_device(R, None, out, ofate, stream))
         c_t = S.last_counts()
         o_t = out.cpu().numpy()
         rel_t = (np.abs(o_t - b) / np.maximum(np.abs(b), 1e-6 * scale)).max(axis=2)
-        pareto.append({"tol_rel": tol, "ms_per_step": ms_t, "speedup_vs_fp64": ms_fp64 / ms_t,
+        pareto.append({"band_scale": shrink, "tol_rel": tol, "ms_per_step": ms_t, "speedup_vs_fp64": ms_fp64 / ms_t,
                        "exact_fraction": c_t["exact"] / max(1, c_t["samples"]),
                        "lit_rel_quantiles_50_90_99_100": [float(x) for x in
                                                           np.quantile(rel_t[lit], [0.5, 0.9, 0.99, 1.0])],
