@@ -29,6 +29,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libgrrt.so")
 
 FORM_FP64 = 0
 FORM_MIXED = 1
+DIAG_HAMILTONIAN = 1
 
 METRIC_SCHWARZSCHILD = 0
 METRIC_KERR = 1
@@ -125,6 +126,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "grrt_render_spectral_cb": (C.c_int, [vp, P(C.c_double), C.c_int, C.c_int, PROGRESS_FN, vp]),
         "grrt_render_spectral_to_fits_cb": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_int, PROGRESS_FN, vp]),
         "grrt_set_precision": (C.c_int, [vp, C.c_int]),
+        "grrt_set_diagnostics": (C.c_int, [vp, C.c_int]),
         "grrt_get_precision": (C.c_int, [vp]),
         "grrt_set_mixed_params": (C.c_int, [vp, C.c_double, C.c_double]),
         "grrt_render_device": (C.c_int, [vp, vp, vp, vp, vp]),
@@ -320,6 +322,9 @@ class Renderer:
     # --- additive API ----------------------------------------------------
     def set_precision(self, form: int) -> None:
         self._check(self._L.grrt_set_precision(self.ctx, form), "grrt_set_precision")
+
+    def set_diagnostics(self, flags: int) -> None:
+        self._check(self._L.grrt_set_diagnostics(self.ctx, flags), "grrt_set_diagnostics")
 
     def set_mixed_params(self, r_factor: float, tol_fp32: float) -> None:
         self._check(self._L.grrt_set_mixed_params(self.ctx, r_factor, tol_fp32), "grrt_set_mixed_params")

@@ -125,6 +125,12 @@ extern "C" GRRT_EXPORT int grrt_render_rows_device(GRRTContext* ctx, int row0, i
     return ctx->render_rgb_device(tile, d_rgba, d_rgb64, d_fate, static_cast<cudaStream_t>(stream), true);
 }
 
+extern "C" GRRT_EXPORT int grrt_set_diagnostics(GRRTContext* ctx, int flags) {
+    if (!ctx || (flags & ~GRRT_DIAG_HAMILTONIAN)) return -1;
+    ctx->diagnostics = flags;
+    return 0;
+}
+
 extern "C" GRRT_EXPORT void grrt_cancel(GRRTContext* ctx) {
     if (ctx) ctx->request_cancel();
 }

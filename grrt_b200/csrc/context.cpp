@@ -59,6 +59,7 @@ GRRTContext::~GRRTContext() {
         for (cudaEvent_t& e : ev_phase)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
+        if (cancel_stream) cudaStreamDestroy(cancel_stream);
         cudaSetDevice(prev);
     }
 }
@@ -278,8 +279,12 @@ bool GRRTContext::ensure_device() {
     if (fail_cuda(cudaMalloc(&d_queue, 256), "cudaMalloc(queue)")) return false;
     if (fail_cuda(cudaMalloc(&d_stats, sizeof(DevStats)), "cudaMalloc(stats)")) return false;
     if (fail_cuda(cudaMemset(d_stats, 0, sizeof(DevStats)), "memset(stats)")) return false;
-    if (fail_cuda(cudaHostAlloc(&h_cancel, sizeof(int), cudaHostAllocMapped), "cudaHostAlloc(cancel)")) return false;
-    *h_cancel = 0;
+    if (fail_cuda(cudaHostAlloc(&h_cancel, 2 * sizeof(int), cudaHostAllocMapped), "cudaHostAlloc(cancel)"))
+        return false;
+    h_cancel[0] = 0;
+    h_cancel[1] = 0x7f7f7f7f;  // beyond any work index; atomic adds after it cannot wrap
+    if (fail_cuda(cudaStreamCreateWithFlags(&cancel_stream, cudaStreamNonBlocking), "cudaStreamCreate(cancel)"))
+        return false;
     if (fail_cuda(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_cancel), h_cancel, 0), "map cancel flag"))
         return false;
     if (fail_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
@@ -310,8 +315,23 @@ DevScene GRRTContext::scene_for_launch() const {
     return S;
 }
 
+// Raises the host-mapped flag (polled by the volumetric kernels, whose long
+// rays must stop mid-trace) and pushes the running launch's work counters past
+// every work index with a copy-engine write (the thin-disk and mixed kernels
+// then take no new work and end once their lanes' current samples end). Safe
+// to call from any thread while a render runs.
 void GRRTContext::request_cancel() {
-    if (h_cancel) *reinterpret_cast<volatile int*>(h_cancel) = 1;
+    if (!h_cancel) return;
+    *reinterpret_cast<volatile int*>(h_cancel) = 1;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    for (unsigned* q : {cancel_q1.load(), cancel_q2.load()})
+        if (q) cudaMemcpyAsync(q, h_cancel + 1, sizeof(unsigned), cudaMemcpyHostToDevice, cancel_stream);
+    cudaGetLastError();
+    cudaSetDevice(prev);
 }
 
 void* GRRTContext::scratch_output(size_t bytes) {
@@ -332,12 +352,15 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
                                    cudaStream_t s, bool reset_stats) {
     if (!ensure_device()) return -1;
     error.clear();
+    // a cancel of an earlier render lands before this one starts
+    cudaStreamSynchronize(cancel_stream);
     *reinterpret_cast<volatile int*>(h_cancel) = 0;
     if (reset_stats && fail_cuda(cudaMemsetAsync(d_stats, 0, sizeof(DevStats), s), "reset stats")) return -1;
     LaunchResources res;
     res.queue = d_queue;
     res.stats = d_stats;
     res.cancel = d_cancel;
+    res.diag_hamiltonian = (diagnostics & GRRT_DIAG_HAMILTONIAN) != 0;
     ThinOutputs out;
     out.rgba = reinterpret_cast<float4*>(d_rgba);
     out.rgb64 = d_rgb64;
@@ -361,6 +384,9 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
                                                : static_cast<unsigned>(tile.w) * tile.h;
     progress_header = (mixed_thin || mixed_vol) ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
     progress_done = vol != nullptr;
+    cancel_q1 = d_queue;
+    cancel_q2 = (mixed_thin || mixed_vol) ? reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_mixed_scratch) + 256)
+                                          : nullptr;
     cudaEventRecord(ev0, s);
     cudaError_t e;
     if (mixed_vol)
@@ -522,6 +548,8 @@ int GRRTContext::render_spectral_tile(const DevTile& tile, double* d_spec, unsig
                                       bool reset_stats) {
     if (!ensure_device()) return -1;
     error.clear();
+    // a cancel of an earlier render lands before this one starts
+    cudaStreamSynchronize(cancel_stream);
     *reinterpret_cast<volatile int*>(h_cancel) = 0;
     const int width = tile.w, height = tile.h;
     const int nb = static_cast<int>(freq_bins.size());
@@ -602,6 +630,8 @@ int GRRTContext::render_spectral_tile(const DevTile& tile, double* d_spec, unsig
                            : static_cast<unsigned>(width) * height;
     progress_header = mixed ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
     progress_done = true;
+    cancel_q1 = d_queue;
+    cancel_q2 = mixed ? reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_mixed_scratch) + 256) : nullptr;
     cudaEventRecord(ev0, s);
     const cudaError_t e =
         mixed ? launch_volume_spectral_mixed(S, tile, d_freqs, nb, out, res, d_mixed_scratch, d_mixed_scratch_bytes,

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <memory>
 #include <string>
 #include <vector>
@@ -37,6 +38,7 @@ struct GRRTContext {
 
     // Precision form and its knobs.
     int form = GRRT_FORM_FP64;
+    int diagnostics = 0;  // GRRT_DIAG_* flags
     double mixed_r_factor = 3.0;
     double tol_fp32 = 3e-6;
     double mixed_margin = 0.05;  // disk-radius margin (M) of the mixed form's re-trace test
@@ -61,8 +63,14 @@ struct GRRTContext {
     grrt_b200::DevScene dev{};
     unsigned int* d_queue = nullptr;
     grrt_b200::DevStats* d_stats = nullptr;
-    int* h_cancel = nullptr;   // host-mapped
-    int* d_cancel = nullptr;   // its device alias
+    int* h_cancel = nullptr;   // host-mapped: [0] the cancel flag, [1] the value a cancel writes to work counters
+    int* d_cancel = nullptr;   // device alias of the flag
+    // work counters of the launch in flight that a cancel pushes past every
+    // work index (the launch's counter; the mixed forms' re-trace counter),
+    // through a host-to-device copy on cancel_stream: the copy engine writes
+    // them while the kernels run, and lanes then take no new work
+    std::atomic<unsigned*> cancel_q1{nullptr}, cancel_q2{nullptr};
+    cudaStream_t cancel_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // per-kernel phases of the last render (thin mixed form: speculate, stars,

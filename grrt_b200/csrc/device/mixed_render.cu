@@ -152,24 +152,6 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 // pass gains more from the fifth block's warps than it loses to the few
 // spilled registers (four blocks: 8.8 ms, five: 8.2 ms on the 1024x1024 4-spp
 // frame on B200; six, with more spills, no better).
-// Warp maximum of the lanes' |H| / p_t^2 into the launch's maximum (the
-// bits of a non-negative double order as integers).
-__device__ __forceinline__ void warp_max_h(DevStats* st, float h) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) h = fmaxf(h, __shfl_xor_sync(kMask, h, o));
-    if ((threadIdx.x & 31u) == 0 && h > 0.0f)
-        atomicMax(&st->h_max_bits, static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(h))));
-}
-
-// True on every lane of the warp once the host has raised the cancel flag
-// (a host-mapped word; lane 0 reads it). Callers poll every 1024 loop
-// iterations, as the FP64 kernels do.
-__device__ __forceinline__ bool cancel_requested(const volatile int* cancel) {
-    int c = 0;
-    if ((threadIdx.x & 31u) == 0) c = *cancel;
-    return __shfl_sync(kMask, c, 0) != 0;
-}
-
 template <bool kBatch>
 __global__ void __launch_bounds__(kMixThreads, 5)
 mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
@@ -189,7 +171,6 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
     bool settled = false;  // black sky, never reaches the disk: final without a trace
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0;
-    unsigned iter = 0;
     mixed::Tracker trk;
     while (true) {
         const bool want = !live && !exhausted;
@@ -229,7 +210,6 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
             }
         }
         if (!__any_sync(kMask, live)) break;
-        if (mb.cancel && ((++iter & 1023u) == 0) && cancel_requested(mb.cancel)) break;
         int term = -1;
         bool retrace = false;
         Vec5<float> k7;
@@ -344,9 +324,7 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
     bool k1_ok = false;
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0, ncross = 0;
-    unsigned iter = 0;
     double c0 = 0, c1 = 0, c2 = 0;
-    float h_max = 0.0f;  // max |H| / p_t^2 at the final state of the lane's samples
     while (true) {
         const bool want = !live && !exhausted;
         const unsigned nq = fetch(want, mb.queue2, total);
@@ -366,7 +344,6 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
             }
         }
         if (!__any_sync(kMask, live)) break;
-        if (mb.cancel && ((++iter & 1023u) == 0) && cancel_requested(mb.cancel)) break;
         int term = -1;
         if (live && retry == 0) term = start_test(S, step, y.r);
         if (live && term < 0) {
@@ -421,9 +398,6 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
         }
         if (live && term >= 0) {
             live = false;
-            if (term != kTermHorizon)  // as the FP64 form: rays that do not end at the horizon
-                h_max = fmaxf(h_max,
-                              static_cast<float>(fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt)));
             if (term == kTermEscaped && S.stars_on) {
                 const double b = star_brightness(S.stars, y.th, y.ph);
                 c0 += b;
@@ -439,7 +413,6 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
     }
 #undef S
     warp_add(stats, n_att, n_acc, 0ull, n_att);
-    warp_max_h(stats, h_max);
 }
 
 // Per pixel: sum the spp sample colours in order, scale, write the outputs.
@@ -622,7 +595,6 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     DevMixedBuffers mb = mixed_buffers(scratch, n, res.queue);
     mb.margin = margin;
     mb.r_near = r_near;
-    mb.cancel = res.cancel;
     cudaError_t e = cudaMemsetAsync(scratch, 0, 1024, stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);

@@ -36,7 +36,6 @@ struct DevMixedBuffers {
     uint32_t* sample_fate = nullptr;    // per sample
     double margin = 0.05;               // disk-radius margin of the re-trace test
     double r_near = 0.0;                // escapes after coming inside r_near are re-traced
-    const volatile int* cancel = nullptr;  // host-mapped cancel flag (single renders), may be null
 };
 
 // Scratch a launch uses beside its inputs and outputs.
@@ -50,6 +49,9 @@ struct LaunchResources {
     // and its scratch, volume_order_bytes(tile); NULL: pixels in index order
     void* order_scratch = nullptr;
     size_t order_scratch_bytes = 0;
+    // thin-disk FP64 form: the diagnostic instantiation that also measures the
+    // Hamiltonian constraint (DevStats::h_max_bits)
+    bool diag_hamiltonian = false;
 };
 
 // Bytes of LaunchResources::order_scratch a volumetric launch over `tile` uses.

@@ -97,7 +97,9 @@ __device__ __forceinline__ int start_check(const DevScene& S, int step, double r
 // kBatch = true: work index -> (chunk, offset) through the batch's chunk table,
 // so one launch covers many cameras (scenes[item.scene]) in the order the
 // schedule lists the chunks.
-template <bool kBatch, int kBlock = kThreads>
+// kDiag: also measure the Hamiltonian constraint at each sample's final state
+// (the diagnostic instantiation; the render instantiation carries no cost).
+template <bool kBatch, int kBlock = kThreads, bool kDiag = false>
 __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B, const DevTile& tile,
                                           float4* __restrict__ out_rgba, double* __restrict__ out_rgb64,
                                           uint32_t* __restrict__ out_fate, unsigned total,
@@ -239,7 +241,7 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
             live = false;
             // the constraint at the final state of rays that do not end at the
             // horizon (there Delta -> 0 and P^2 / Delta cancels catastrophically)
-            if (term != kTermHorizon)
+            if (kDiag && term != kTermHorizon)
                 cold.h_max = fmax(cold.h_max, fabs(kerr_hamiltonian<double>(S.M, S.a, pt, pph, y)) / (pt * pt));
             double c0 = cold.col[0], c1 = cold.col[1], c2 = cold.col[2];
             if (term == kTermEscaped) {
@@ -299,13 +301,15 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
     flush_counters(stats, n_attempts, n_accepted, cold, cancelled);
 }
 
+template <bool kDiag>
 __global__ void __launch_bounds__(kThreads, GRRT_THIN_MIN_BLOCKS)
 thin_render_kernel(const __grid_constant__ DevScene S, const DevTile tile, float4* __restrict__ out_rgba,
                    double* __restrict__ out_rgb64, uint32_t* __restrict__ out_fate,
                    unsigned int* __restrict__ queue, DevStats* __restrict__ stats,
                    const volatile int* __restrict__ cancel) {
     const unsigned total = static_cast<unsigned>(tile.w) * static_cast<unsigned>(tile.h);
-    thin_loop<false>(S, DevBatch{}, tile, out_rgba, out_rgb64, out_fate, total, queue, stats, cancel);
+    thin_loop<false, kThreads, kDiag>(S, DevBatch{}, tile, out_rgba, out_rgb64, out_fate, total, queue, stats,
+                                      cancel);
 }
 
 // One launch over many cameras: the batched form. Work index space =
@@ -328,7 +332,7 @@ cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutput
     const Shape& sh = per_device_shape<Shape>([](int dev) {
         Shape v;
         cudaDeviceGetAttribute(&v.sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.per, thin_render_kernel, kThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.per, thin_render_kernel<false>, kThreads, 0);
         if (v.per < 1) v.per = 1;
         return v;
     });
@@ -340,8 +344,12 @@ cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutput
     if (needed < blocks) blocks = needed;
     cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    thin_render_kernel<<<blocks, kThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
-                                                        res.stats, res.cancel);
+    if (res.diag_hamiltonian)
+        thin_render_kernel<true><<<blocks, kThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
+                                                                  res.stats, res.cancel);
+    else
+        thin_render_kernel<false><<<blocks, kThreads, 0, stream>>>(S, tile, out.rgba, out.rgb64, out.fate, res.queue,
+                                                                   res.stats, res.cancel);
     return cudaGetLastError();
 }
 

@@ -47,12 +47,21 @@ typedef struct {
     unsigned long long bin_updates;   /* per-frequency transfer updates */
     unsigned long long fp64_attempts; /* attempts evaluated in FP64 */
     double kernel_ms;                 /* device time of the render kernels (CUDA events) */
-    double hamiltonian_max;           /* thin-disk FP64 traces (FP64 form, the mixed form's
-                                         re-trace): max over the samples that do not end at the
-                                         horizon of |H| / p_t^2 at the final state,
-                                         H = 1/2 g^{mu nu} p_mu p_nu (0 on the light cone; near the
-                                         horizon its evaluation cancels); 0 where not measured */
+    double hamiltonian_max;           /* with GRRT_DIAG_HAMILTONIAN, thin-disk FP64 form: max over
+                                         the samples that do not end at the horizon of |H| / p_t^2
+                                         at the final state, H = 1/2 g^{mu nu} p_mu p_nu (0 on the
+                                         light cone; near the horizon its evaluation cancels);
+                                         0 where not measured */
 } GRRTStats;
+
+/* Diagnostics of later renders (flags, 0 = none). GRRT_DIAG_HAMILTONIAN: the
+ * thin-disk FP64 form runs its diagnostic instantiation, which also measures
+ * the Hamiltonian constraint at every sample's final state
+ * (GRRTStats.hamiltonian_max); the render itself is unchanged. No counterpart
+ * in the reference (its README says the constraint is monitored). Returns 0,
+ * or -1 for unknown flags. */
+#define GRRT_DIAG_HAMILTONIAN 1
+GRRT_EXPORT int grrt_set_diagnostics(GRRTContext* ctx, int flags);
 
 /* Select the precision form for later renders (src/geodesic_tracer.cpp:100 is
  * the FP64 call it replaces). Returns 0, or -1 for an unknown form. */

@@ -5,8 +5,8 @@ rounding-sensitive ("caustic") band from the oracle itself.
 Image-integrated flux. The volumetric march amplifies rounding: the probes
 move a volumetric frame's flux per bin by ~1e-3 relative (the reference's own
 strict and as-shipped builds differ per pixel by a median of ~5%), so the
-flux bar of a device render is data-driven: within twice the largest move of
-any probe (OracleRGB / OracleSpectral.probe_flux_spread).
+flux bar of a device render is data-driven: within a few times the largest
+move of any probe (OracleRGB / OracleSpectral.probe_flux_spread).
 
 Band definition. A sample is rounding-sensitive when the strict oracle and a
 rounding-level probe disagree on the fate or differ by more than the test

@@ -2,8 +2,10 @@
 
 The reference's CPU versions are stubs (src/api.cpp:220-231: cancel does
 nothing, progress returns 1.0); its CUDA backend cancels through a host-mapped
-flag (cuda/cuda_backend.cu:31-34). Here the flag is host-mapped pinned memory
-that the render kernels poll every 1024 loop iterations per warp, and the
+flag (cuda/cuda_backend.cu:31-34). Here a cancel raises a host-mapped flag,
+which the volumetric kernels poll every 1024 loop iterations per warp, and
+pushes the running launch's work counters past every work index with a
+copy-engine write, so the thin-disk and mixed kernels take no new work. The
 progress callback fires on the calling thread while the render runs.
 
 No device fault is involved: the cancel is a plain host write that the

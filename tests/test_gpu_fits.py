@@ -14,9 +14,9 @@ and odd image sizes; 1 and 4 spp):
     oracle's probes, tests/parity_util.py) at least 99% of the pixels are
     within 1e-9 relative and every one within 1e-6; every pixel lies within
     1e-6 of the range that the oracle and its rounding probes span, or the
-    band holds it; the image-integrated flux per bin is within twice the move
-    that the rounding-level probes themselves make in it (the volumetric march
-    amplifies rounding: the probes move it by ~1e-3).
+    band holds it; the image-integrated flux per bin is within four times the
+    largest move that the five rounding-level probes themselves make in it (the
+    volumetric march amplifies rounding: the probes move it by ~1e-3).
 """
 import json
 import os
@@ -85,7 +85,7 @@ def test_fits_file_matches_reference(grrt, need_gpu, golden, tmp_path, case):
     worst = float(np.max(err[out])) if out.any() else 0.0
     herr = hull_error(got, orc.pixel_lo, orc.pixel_hi)
     ferr = flux_spread(got, want)
-    fbar = max(1e-9, 2.0 * orc.probe_flux_spread)
+    fbar = max(1e-9, 4.0 * orc.probe_flux_spread)
     print(f"\n  [{case}] band {orc.pixel_band.mean():.4f}; outside band within {TOL}: {within:.5f}, worst "
           f"{worst:.2e}; outside the probe range by > {LOOSE}: {int(np.sum(herr > LOOSE))} pixels "
           f"(max {herr.max():.2e}); integrated flux per bin: max rel err {ferr:.2e} (probes move it by "
