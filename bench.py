@@ -68,6 +68,17 @@ RAYS = W * H * SPP
 # F_EVAL per ray).
 F_EVAL = 133 + 37
 F_ATTEMPT_EXEC = 6 * F_EVAL + 480
+# Operations the kernels execute per attempt (all of a kernel's floating-point
+# operations divided by its attempts; a fused multiply-add counts 2), from the
+# ncu instruction counters of a 512x512 4-spp frame
+# (profiles/executed_flops_thin_mixed_kernels_kerr_512x512_4spp.md): the FP64
+# kernels (thin_render_kernel, mixed_retrace_kernel) and the FP32 speculation
+# (packed two-wide instructions count once there: a lower bound).
+F_EXEC_FP64_ATTEMPT = 1022.8
+F_EXEC_FP32_ATTEMPT = 479.4
+# DRAM bytes (read + write) of one mixed_speculate_kernel launch on the
+# 1024x1024 4-spp frame, from ncu (None until captured)
+TRAFFIC_SPECULATE_C2 = None
 
 
 def parse():
@@ -803,6 +814,10 @@ def main():
         a64 = fl64 / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
         forms["fp64"]["roofline"] = {"kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": a64,
                                      "peak": p64, "unit": "TFLOP/s", "frac": a64 / p64}
+        e64 = st64["attempts"] * F_EXEC_FP64_ATTEMPT / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
+        forms["fp64"]["roofline_executed"] = {
+            "kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": e64, "peak": p64, "unit": "TFLOP/s",
+            "frac": e64 / p64, "flop_count": f"{F_EXEC_FP64_ATTEMPT} executed FP64 flop per attempt (ncu counters)"}
         # mixed form: the speculation kernel (FP32 FLOPs vs the SGEMM peak) and
         # the re-trace kernel (FP64 FLOPs vs the DGEMM peak)
         stm = res[G.FORM_MIXED]["stats"]
@@ -815,6 +830,13 @@ def main():
         forms["mixed"]["roofline"] = {
             "speculate": {"bound": "fp32", "achieved": a_spec, "peak": p32, "unit": "TFLOP/s", "frac": a_spec / p32},
             "retrace": {"bound": "fp64", "achieved": a_re, "peak": p64, "unit": "TFLOP/s", "frac": a_re / p64}}
+        x_spec = spec_att * F_EXEC_FP32_ATTEMPT / (ph[0] * 1e-3) / 1e12
+        x_re = stm["fp64_attempts"] * F_EXEC_FP64_ATTEMPT / (ph[2] * 1e-3) / 1e12
+        forms["mixed"]["roofline_executed"] = {
+            "speculate": {"bound": "fp32", "achieved": x_spec, "peak": p32, "unit": "TFLOP/s", "frac": x_spec / p32,
+                          "flop_count": f"{F_EXEC_FP32_ATTEMPT} executed FP32 flop per attempt (ncu; lower bound)"},
+            "retrace": {"bound": "fp64", "achieved": x_re, "peak": p64, "unit": "TFLOP/s", "frac": x_re / p64,
+                        "flop_count": f"{F_EXEC_FP64_ATTEMPT} executed FP64 flop per attempt (ncu counters)"}}
         if head_form == G.FORM_MIXED:
             roof = dict(forms["mixed"]["roofline"]["speculate"])
             roof.update(kernel="mixed_speculate_kernel", flops_per_launch=spec_att * F_ATTEMPT_EXEC + my_rays * F_EVAL,
@@ -823,7 +845,9 @@ def main():
                                    f"+ {F_EVAL} per ray",
                         peak_source="cuBLAS SGEMM 8192^3, TF32 off, measured in this run (best of 5); "
                                     "MEASURED_PEAKS.json has no FP32 figure",
-                        launch_ms=ph[0], traffic=None)
+                        launch_ms=ph[0], executed=forms["mixed"]["roofline_executed"]["speculate"],
+                        # DRAM bytes of one full-size launch: profiles/ (ncu, a single-pass metric pair)
+                        traffic=TRAFFIC_SPECULATE_C2)
             launches = args.steps * (4 if params["background_type"] == G.BG_STARS else 3)
         else:
             roof = dict(forms["fp64"]["roofline"])

@@ -49,7 +49,6 @@ GRRTContext::~GRRTContext() {
         cudaFree(d_freqs);
         cudaFree(d_spec_scratch);
         cudaFree(d_mixed_scratch);
-        cudaFree(d_order);
         if (h_cancel) cudaFreeHost(h_cancel);
         if (h_stage) cudaFreeHost(h_stage);
         for (cudaEvent_t& e : ev_copy)
@@ -594,22 +593,12 @@ int GRRTContext::render_spectral_tile(const DevTile& tile, double* d_spec, unsig
         if (fail_cuda(cudaMalloc(&d_spec_scratch, need * sizeof(double)), "cudaMalloc(spectral scratch)")) return -1;
         d_spec_scratch_n = need;
     }
-    const size_t ob = volume_order_bytes(tile);
-    if (ob > d_order_bytes) {
-        cudaFree(d_order);
-        d_order = nullptr;
-        d_order_bytes = 0;
-        if (fail_cuda(cudaMalloc(&d_order, ob), "cudaMalloc(order)")) return -1;
-        d_order_bytes = ob;
-    }
     LaunchResources res;
     res.queue = d_queue;
     res.stats = d_stats;
     res.cancel = d_cancel;
     res.spectral_scratch = d_spec_scratch;
     res.spectral_scratch_elems = d_spec_scratch_n;
-    res.order_scratch = d_order;
-    res.order_scratch_bytes = d_order_bytes;
     SpectralOutputs out;
     out.spec = d_spec;
     out.fate = d_fate;

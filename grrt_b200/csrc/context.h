@@ -92,8 +92,6 @@ struct GRRTContext {
     size_t d_spec_scratch_n = 0;
     void* d_mixed_scratch = nullptr;
     size_t d_mixed_scratch_bytes = 0;
-    void* d_order = nullptr;  // volumetric FP64 forms: longest-first pixel order and its scratch
-    size_t d_order_bytes = 0;
 
     GRRTContext() = default;
     ~GRRTContext();

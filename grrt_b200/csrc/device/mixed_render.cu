@@ -485,8 +485,14 @@ static size_t mixed_order_offset(size_t n_samples) {
     return ((n_samples * (3 * sizeof(double) + 3 * sizeof(unsigned)) + 1024 + 255) / 256) * 256;
 }
 
+// the longest-first re-trace list (black sky) and its ordering scratch
+static size_t mixed_cost_offset(size_t n_samples) {
+    return mixed_order_offset(n_samples) + ((order_list_scratch_bytes(n_samples) + 255) / 256) * 256;
+}
+
 size_t mixed_scratch_bytes_for(size_t n_samples) {
-    return mixed_order_offset(n_samples) + order_list_scratch_bytes(n_samples);
+    return mixed_cost_offset(n_samples) + ((n_samples * sizeof(unsigned) + 255) / 256) * 256 +
+           cost_order_scratch_bytes(n_samples);
 }
 
 void* mixed_order_scratch(void* scratch, size_t n_samples) {
@@ -562,9 +568,27 @@ cudaError_t launch_mixed_stars(const DevScene& S, const DevTile& tile, const Dev
 }
 
 cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
-                                 cudaStream_t stream) {
+                                 void* scratch, cudaStream_t stream) {
     const MixLaunchShape& sh = mix_shape();
-    mixed_retrace_kernel<false><<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, mb, stats);
+    DevMixedBuffers m = mb;
+    if (!S.stars_on) {
+        // Black sky: the list holds lit samples near the hole, whose lengths
+        // follow their closed-form distance to the critical curve; taken
+        // nearest first, the long ones start first (the C5 frame, 2048^2 at
+        // a = 0.998: re-trace 5.47 -> 5.02 ms on B200). Under a star sky the
+        // list is mostly escapes with a star in reach, and the finding order,
+        // which groups rays of similar length into warps, is faster (1024^2
+        // 4-spp frame: 7.58 against 8.43 ms ordered).
+        const size_t n = static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid;
+        auto* base = static_cast<unsigned char*>(scratch) + mixed_cost_offset(n);
+        auto* ordered = reinterpret_cast<unsigned*>(base);
+        void* cs = base + ((n * sizeof(unsigned) + 255) / 256) * 256;
+        const cudaError_t e =
+            order_by_cost(S, tile, mb.retrace_list, static_cast<unsigned>(n), mb.retrace_count, true, ordered, cs, stream);
+        if (e != cudaSuccess) return e;
+        m.retrace_list = ordered;
+    }
+    mixed_retrace_kernel<false><<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, m, stats);
     return cudaGetLastError();
 }
 
@@ -606,7 +630,7 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     e = launch_mixed_stars(S, tile, mb, stream);
     if (e != cudaSuccess) return e;
     mark(2);
-    e = launch_mixed_retrace(S, tile, mb, stats, stream);
+    e = launch_mixed_retrace(S, tile, mb, stats, scratch, stream);
     if (e != cudaSuccess) return e;
     mark(3);
     e = launch_mixed_resolve(S, tile, mb, out, stats, stream);

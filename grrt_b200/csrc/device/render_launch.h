@@ -45,17 +45,10 @@ struct LaunchResources {
     const volatile int* cancel = nullptr;  // host-mapped cancel flag, may be null
     double* spectral_scratch = nullptr;    // spectral transfer state, see volume_spectral_scratch_elems
     size_t spectral_scratch_elems = 0;
-    // volumetric FP64 forms: the longest-first pixel order (order_by_cost)
-    // and its scratch, volume_order_bytes(tile); NULL: pixels in index order
-    void* order_scratch = nullptr;
-    size_t order_scratch_bytes = 0;
     // thin-disk FP64 form: the diagnostic instantiation that also measures the
     // Hamiltonian constraint (DevStats::h_max_bits)
     bool diag_hamiltonian = false;
 };
-
-// Bytes of LaunchResources::order_scratch a volumetric launch over `tile` uses.
-size_t volume_order_bytes(const DevTile& tile);
 
 // Longest-first order of n work items (cost_order.cu): items (NULL: 0..n-1;
 // the count may be on the device, n_dev, at most n) are pixels of the tile
@@ -135,8 +128,10 @@ cudaError_t launch_mixed_speculate(const DevScene& S, const DevTile& tile, const
                                    DevStats* stats, cudaStream_t stream);
 cudaError_t launch_mixed_stars(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
                                cudaStream_t stream);
+// scratch: the mixed scratch the buffers were cut from (mixed_scratch_bytes);
+// on a black sky the list is ordered longest first in its tail region.
 cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
-                                 cudaStream_t stream);
+                                 void* scratch, cudaStream_t stream);
 cudaError_t launch_mixed_resolve(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb,
                                  const ThinOutputs& out, DevStats* stats, cudaStream_t stream);
 

@@ -126,8 +126,6 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
     double pt = 0.0, pph = 0.0;
     double dl = 0.0;
     int retry = 0, step = 0;
-    bool cancelled = false;
-    unsigned iter = 0;
 
     while (true) {
         // ---- refill: lanes without a pixel take one (warp-aggregated atomic) ----
@@ -284,21 +282,13 @@ __device__ __forceinline__ void thin_loop(const DevScene& S0, const DevBatch& B,
             }
         }
 
-        // ---- cancellation (host-mapped flag, polled by one lane per warp) ----
-        if (cancel && ((++iter & 1023u) == 0)) {
-            int c = 0;
-            if (lane == 0) c = *cancel;
-            c = __shfl_sync(kFull, c, 0);
-            if (c) {
-                cancelled = true;
-                break;
-            }
-        }
+        // (no polling for a cancel: grrt_cancel pushes the work counter past
+        // every pixel, and the lanes end with their current samples)
         // ---- exit when the queue is drained and no lane holds a ray ----
         if (!__any_sync(kFull, live || pix >= -1)) break;
     }
 #undef S
-    flush_counters(stats, n_attempts, n_accepted, cold, cancelled);
+    flush_counters(stats, n_attempts, n_accepted, cold, false);
 }
 
 template <bool kDiag>

@@ -53,10 +53,9 @@ constexpr unsigned kWarp = 0xffffffffu;
 
 }  // namespace
 
-// kList = false: work item = pixel of the tile (list[k] when list is given:
-// the longest-first pixel order of order_by_cost); its spp samples are traced
-// in order, summed in the row's pixel-sum part, and out_spec[pixel][nb] is
-// written. kList = true: work item k = sample list[k] (pixel * grid^2 + s)
+// kList = false: work item = pixel of the tile (list[k] when a pixel order
+// is given); its spp samples are traced in order, summed in the row's
+// pixel-sum part, and out_spec[pixel][nb] is written. kList = true: work item k = sample list[k] (pixel * grid^2 + s)
 // of the tile; out_spec[sample][nb] receives the sample's J (its term of the
 // pixel sum is J nu^3).
 // kBatch = true (with kList = false): the batched form over many volumetric
@@ -718,24 +717,8 @@ cudaError_t launch_volume_spectral(const DevScene& S, const DevTile& tile, const
     // work counter and finished-items counter
     cudaError_t e = cudaMemsetAsync(res.queue, 0, 2 * sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    // longest rays first
-    unsigned* order = nullptr;
-    if (res.order_scratch && res.order_scratch_bytes >= volume_order_bytes(tile)) {
-        order = static_cast<unsigned*>(res.order_scratch);
-        e = order_by_cost(S, tile, nullptr, total, nullptr, false, order,
-                          static_cast<unsigned char*>(res.order_scratch) + ((total * sizeof(unsigned) + 255) / 256) * 256,
-                          stream);
-        if (e != cudaSuccess) return e;
-    }
-    vol_spectral_kernel<false><<<blocks, kSpecThreads, 0, stream>>>(S, tile, freqs, nb, out.spec, out.fate,
-                                                                     res.spectral_scratch, res.queue, res.stats,
-                                                                     res.cancel, order, nullptr, DevBatch{});
-    return cudaGetLastError();
-}
-
-size_t volume_order_bytes(const DevTile& tile) {
-    const size_t n = static_cast<size_t>(tile.w) * tile.h;
-    return ((n * sizeof(unsigned) + 255) / 256) * 256 + cost_order_scratch_bytes(n);
+    return launch_vol_spectral_on(S, tile, freqs, nb, out.spec, out.fate, res.spectral_scratch, res.queue, res.stats,
+                                  res.cancel, blocks, stream);
 }
 
 int vol_spectral_batch_max_blocks_per_sm() {
@@ -764,9 +747,9 @@ cudaError_t launch_vol_spectral_batch(const DevBatch& B, int nb_max, double* out
 size_t volume_mixed_scratch_bytes(const DevTile& tile, int g2, int nb) {
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
     // header (counters), the re-trace list (rounded up to 256 B), per-sample J
-    // (rounded up to 256 B), the ordered list and the ordering's scratch
-    return 1024 + 2 * ((n * sizeof(unsigned) + 255) / 256) * 256 + ((n * nb * sizeof(double) + 255) / 256) * 256 +
-           cost_order_scratch_bytes(n);
+    // (rounded up to 256 B), the list ordering's bitmap and block sums
+    return 1024 + ((n * sizeof(unsigned) + 255) / 256) * 256 + ((n * nb * sizeof(double) + 255) / 256) * 256 +
+           order_list_scratch_bytes(n);
 }
 
 cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile, const double* freqs, int nb,
@@ -786,10 +769,9 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     unsigned* list_count = reinterpret_cast<unsigned*>(base + 512);
     unsigned* list = reinterpret_cast<unsigned*>(base + 1024);
     auto* sample_spec = reinterpret_cast<double*>(base + 1024 + ((n * sizeof(unsigned) + 255) / 256) * 256);
-    auto* ordered = reinterpret_cast<unsigned*>(reinterpret_cast<unsigned char*>(sample_spec) +
-                                                ((n * nb * sizeof(double) + 255) / 256) * 256);
-    unsigned char* order_scratch = reinterpret_cast<unsigned char*>(ordered) + ((n * sizeof(unsigned) + 255) / 256) * 256;
-    if (static_cast<size_t>(order_scratch - base) + cost_order_scratch_bytes(n) > scratch_bytes)
+    unsigned char* order_scratch =
+        reinterpret_cast<unsigned char*>(sample_spec) + ((n * nb * sizeof(double) + 255) / 256) * 256;
+    if (static_cast<size_t>(order_scratch - base) + order_list_scratch_bytes(n) > scratch_bytes)
         return cudaErrorInvalidValue;
     int lb = sh.sms * sh.per_list;
     if (!res.spectral_scratch || res.spectral_scratch_elems < static_cast<size_t>(4) * nb * lb * kSpecThreads)
@@ -809,14 +791,14 @@ cudaError_t launch_volume_spectral_mixed(const DevScene& S, const DevTile& tile,
     vol_speculate_kernel<false><<<sb, kSpecThreads, 0, stream>>>(S, tile, reach, out.fate, res.queue, list,
                                                                 list_count, nullptr, res.stats);
     e = cudaGetLastError();
-    // the re-trace takes its samples longest first (as the FP64 form its pixels)
-    if (e == cudaSuccess)
-        e = order_by_cost(S, tile, list, static_cast<unsigned>(n), list_count, true, ordered, order_scratch, stream);
+    // the re-trace takes its samples in the FP64 form's order (the speculation
+    // lists them in the order it finds them, the longest last)
+    if (e == cudaSuccess) e = order_sample_list(list, list_count, n, order_scratch, stream);
     if (e != cudaSuccess) return e;
     mark(1);
     vol_spectral_kernel<true><<<lb, kSpecThreads, 0, stream>>>(S, tile, freqs, nb, sample_spec, out.fate,
                                                                 res.spectral_scratch, queue2, res.stats, res.cancel,
-                                                                ordered, list_count, DevBatch{});
+                                                                list, list_count, DevBatch{});
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     mark(2);

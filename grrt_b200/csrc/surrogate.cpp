@@ -545,7 +545,8 @@ struct GRRTSurrogate {
             fail(launch_mixed_stars(S, tile, mb, stream), "star pass"))
             return false;
         cudaEventRecord(ctx->ev_phase[2], stream);
-        if (fail(launch_mixed_retrace(S, tile, mb, ctx->d_stats, stream), "exact re-trace")) return false;
+        if (fail(launch_mixed_retrace(S, tile, mb, ctx->d_stats, ctx->d_mixed_scratch, stream), "exact re-trace"))
+            return false;
         cudaEventRecord(ctx->ev_phase[3], stream);
         ThinOutputs out;
         out.rgba = reinterpret_cast<float4*>(d_rgba);
