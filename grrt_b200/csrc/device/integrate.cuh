@@ -59,50 +59,6 @@ template <typename T>
 GRRT_HD T dp45_attempt_k1(T M, T a, T pt, T pph, const Vec5<T>& y, T h, const Vec5<T>& k1, Vec5<T>& y5,
                           Vec5<T>& k7_out) {
     using namespace dp;
-#ifdef GRRT_DP45_CARRIED
-    // Each stage input y + h * (sum_j a_sj k_j), the 5th-order sum
-    // sum_j b_j k_j and the error sum sum_j e_j k_j are accumulated in the
-    // tableau's order, left to right. Stages 2-5 read the kept k's; from k4
-    // on, the sums that later stages, y5 and the error need are carried
-    // instead (three vectors: the stage-6 sum, the 5th-order sum and the
-    // error sum), so no more than three stage vectors are live across a
-    // right-hand-side evaluation. The order of every addition is that of the
-    // written-out sums.
-#define GRRT_S2(f) y.f + h * (T(a21) * k1.f)
-    const Vec5<T> k2 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{GRRT_S2(r), GRRT_S2(th), GRRT_S2(ph), GRRT_S2(pr), GRRT_S2(pth)});
-#define GRRT_S3(f) y.f + h * (T(a31) * k1.f + T(a32) * k2.f)
-    const Vec5<T> k3 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{GRRT_S3(r), GRRT_S3(th), GRRT_S3(ph), GRRT_S3(pr), GRRT_S3(pth)});
-#define GRRT_S4(f) y.f + h * (T(a41) * k1.f + T(a42) * k2.f + T(a43) * k3.f)
-    const Vec5<T> k4 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{GRRT_S4(r), GRRT_S4(th), GRRT_S4(ph), GRRT_S4(pr), GRRT_S4(pth)});
-    // carried sums over k1..k4
-#define GRRT_P6(f) (T(a61) * k1.f + T(a62) * k2.f + T(a63) * k3.f + T(a64) * k4.f)
-#define GRRT_PB(f) (T(b1) * k1.f + T(b3) * k3.f + T(b4) * k4.f)
-#define GRRT_PE(f) (T(e1) * k1.f + T(e3) * k3.f + T(e4) * k4.f)
-    Vec5<T> p6{GRRT_P6(r), GRRT_P6(th), GRRT_P6(ph), GRRT_P6(pr), GRRT_P6(pth)};
-    Vec5<T> pb{GRRT_PB(r), GRRT_PB(th), GRRT_PB(ph), GRRT_PB(pr), GRRT_PB(pth)};
-    Vec5<T> pe{GRRT_PE(r), GRRT_PE(th), GRRT_PE(ph), GRRT_PE(pr), GRRT_PE(pth)};
-#define GRRT_S5(f) y.f + h * (T(a51) * k1.f + T(a52) * k2.f + T(a53) * k3.f + T(a54) * k4.f)
-    const Vec5<T> k5 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{GRRT_S5(r), GRRT_S5(th), GRRT_S5(ph), GRRT_S5(pr), GRRT_S5(pth)});
-#define GRRT_ADD(v, c, k) v = Vec5<T>{v.r + T(c) * k.r, v.th + T(c) * k.th, v.ph + T(c) * k.ph, v.pr + T(c) * k.pr, \
-                                      v.pth + T(c) * k.pth}
-    GRRT_ADD(p6, a65, k5);
-    GRRT_ADD(pb, b5, k5);
-    GRRT_ADD(pe, e5, k5);
-    const Vec5<T> k6 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{y.r + h * p6.r, y.th + h * p6.th, y.ph + h * p6.ph,
-                                                          y.pr + h * p6.pr, y.pth + h * p6.pth});
-    GRRT_ADD(pb, b6, k6);
-    GRRT_ADD(pe, e6, k6);
-    y5 = Vec5<T>{y.r + h * pb.r, y.th + h * pb.th, y.ph + h * pb.ph, y.pr + h * pb.pr, y.pth + h * pb.pth};
-    const Vec5<T>& e = pe;
-#undef GRRT_S2
-#undef GRRT_S3
-#undef GRRT_S4
-#undef GRRT_S5
-#undef GRRT_P6
-#undef GRRT_PB
-#undef GRRT_PE
-#undef GRRT_ADD
-#else
 #define GRRT_S2(f) y.f + h * (T(a21) * k1.f)
     const Vec5<T> k2 = kerr_rhs<T>(M, a, pt, pph, Vec5<T>{GRRT_S2(r), GRRT_S2(th), GRRT_S2(ph), GRRT_S2(pr), GRRT_S2(pth)});
 #define GRRT_S3(f) y.f + h * (T(a31) * k1.f + T(a32) * k2.f)
@@ -124,7 +80,6 @@ GRRT_HD T dp45_attempt_k1(T M, T a, T pt, T pph, const Vec5<T>& y, T h, const Ve
 #undef GRRT_S6
 #undef GRRT_Y5
 #undef GRRT_E6
-#endif
     const Vec5<T> k7 = kerr_rhs<T>(M, a, pt, pph, y5);
     k7_out = k7;
     // err = max |h (sum e_i k_i)| / (|y5| + 1e-10); max written as the
