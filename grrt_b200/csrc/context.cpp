@@ -367,8 +367,11 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     const DevScene S = scene_for_launch();
     const bool mixed_thin = !vol && form == GRRT_FORM_MIXED;
     const bool mixed_vol = vol && form == GRRT_FORM_MIXED;
+    // the thin-disk FP64 form traces by samples into the same per-sample
+    // buffers (the Hamiltonian diagnostic keeps the per-pixel kernel)
+    const bool fp64_thin = !vol && !mixed_thin && !res.diag_hamiltonian;
     size_t mixed_bytes = 0;
-    if (mixed_thin || mixed_vol) {
+    if (mixed_thin || mixed_vol || fp64_thin) {
         mixed_bytes = mixed_scratch_bytes(tile, S.grid * S.grid);
         if (mixed_bytes > d_mixed_scratch_bytes) {
             cudaFree(d_mixed_scratch);
@@ -379,8 +382,9 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
         }
     }
     n_phases = 0;
-    progress_total = (mixed_thin || mixed_vol) ? static_cast<unsigned>(tile.w) * tile.h * (S.grid * S.grid)
-                                               : static_cast<unsigned>(tile.w) * tile.h;
+    progress_total = (mixed_thin || mixed_vol || fp64_thin)
+                         ? static_cast<unsigned>(tile.w) * tile.h * (S.grid * S.grid)
+                         : static_cast<unsigned>(tile.w) * tile.h;
     progress_header = (mixed_thin || mixed_vol) ? static_cast<const unsigned char*>(d_mixed_scratch) : nullptr;
     progress_done = vol != nullptr;
     cancel_q1 = d_queue;
@@ -396,6 +400,8 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
     else if (mixed_thin)
         e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
                               mixed_r_near(), ev_phase, s);
+    else if (fp64_thin)
+        e = launch_thin_fp64(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, s);
     else
         e = launch_thin(S, tile, out, res, s);
     cudaEventRecord(ev1, s);

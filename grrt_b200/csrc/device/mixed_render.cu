@@ -310,47 +310,140 @@ mixed_star_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const
 }
 
 // FP64 re-trace of the queued samples with the plain form's arithmetic.
+namespace {
+
+// Per-warp staging of the FP64 trace in shared memory, one slot per lane,
+// fields stored as arrays so that lane k touches element k (no bank
+// conflicts beyond the two wavefronts of an 8-byte access).
+//   Prepared starts: the warp takes 32 work items at once and every lane
+//   forms one item's camera ray and the first stage f(y) of its first
+//   attempt, so this work runs with the whole warp instead of one lane at a
+//   time as rays end; lanes whose ray ended take the slots in order.
+//   Deferred star lookups: an escape under a star sky parks its direction and
+//   colour here, and the warp looks up up to 32 of them at once.
+struct WarpStage {
+    double pr[32], pth[32], pt[32], pph[32];  // start momentum (r, theta, phi are the camera's)
+    double k[5][32];                          // f(y) at the start
+    unsigned q[32];                           // sample index
+    const DevScene* sp[32];                   // batch: the sample's scene
+    double th[32], ph[32], c[3][32];          // escape direction and colour so far
+    unsigned pq[32], pfate[32];
+    const DevScene* psp[32];
+};
+
+// Writes the parked escapes' colours (colour + star brightness, the order of
+// the single-lane form) and fate words; lanes below n each take one.
 template <bool kBatch>
+__device__ __forceinline__ void flush_star_lookups(WarpStage& W, int n, const DevScene& S0,
+                                                   const DevMixedBuffers& mb) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < n) {
+        const DevScene& Sl = kBatch ? *W.psp[lane] : S0;
+        const double b = star_brightness(Sl.stars, W.th[lane], W.ph[lane]);
+        const size_t q = W.pq[lane];
+        mb.sample_rgb[3 * q + 0] = W.c[0][lane] + b;
+        mb.sample_rgb[3 * q + 1] = W.c[1][lane] + b;
+        mb.sample_rgb[3 * q + 2] = W.c[2][lane] + b;
+        mb.sample_fate[q] = W.pfate[lane];
+    }
+    __syncwarp();
+}
+
+}  // namespace
+
+// FP64 trace of samples into per-sample colours and fate words, the plain
+// method of GeodesicTracer::trace (src/geodesic_tracer.cpp:23-181): the FP64
+// form traces every sample of the tile (kList = false, work item = sample),
+// the mixed form's re-trace the listed ones (kList = true, work item = entry
+// of mb.retrace_list). Each loop iteration is one DP45 attempt for every lane
+// with a live ray. The per-sample work around it (camera ray, first
+// right-hand side, star lookup) runs for 32 samples at a time with the whole
+// warp (WarpStage), not lane by lane as rays end. counter: the work counter
+// (zeroed by the launcher), total: the item count for kList = false.
+template <bool kList, bool kBatch>
 __global__ void __launch_bounds__(kMixThreads, 4)
-mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
-                     DevMixedBuffers mb, DevStats* stats) {
+fp64_trace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
+                  DevMixedBuffers mb, unsigned* __restrict__ counter, unsigned total_items, DevStats* stats) {
+    __shared__ WarpStage stage_all[kMixThreads / 32];
+    WarpStage& W = stage_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
     const DevScene* sp = nullptr;
 #define S (kBatch ? *sp : S0)
-    const unsigned total = *mb.retrace_count;
-    unsigned long long n_att = 0, n_acc = 0;
-    unsigned q = ~0u;
-    bool live = false, exhausted = false;
-    Vec5<double> y, k1;  // k1 = f(y), kept from the previous attempt when k1_ok
-    bool k1_ok = false;
+    const unsigned total = kList ? *mb.retrace_count : total_items;
+    unsigned long long n_att = 0, n_acc = 0, n_rays = 0;
+    // warp-uniform: prepared slots [ring_head, ring_n), parked lookups, queue state
+    int ring_head = 0, ring_n = 0, pend_n = 0;
+    bool drained = false;
+    unsigned q = 0;
+    bool live = false;
+    Vec5<double> y, k1;  // k1 = f(y)
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0, ncross = 0;
     double c0 = 0, c1 = 0, c2 = 0;
     while (true) {
-        const bool want = !live && !exhausted;
-        const unsigned nq = fetch(want, mb.queue2, total);
-        if (want) {
-            if (nq == ~0u) {
-                exhausted = true;
-            } else {
-                q = mb.retrace_list[nq];
-                start_ray<kBatch>(S0, tile, B, q, sp, y, pt, pph);
+        const unsigned need = __ballot_sync(kMask, !live);
+        // ---- the warp prepares its next 32 starts (every lane one) ----
+        if (need && ring_head == ring_n && !drained) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(counter, 32u);
+            base = __shfl_sync(kMask, base, 0);
+            ring_head = 0;
+            ring_n = base < total ? static_cast<int>(min(32u, total - base)) : 0;
+            if (ring_n < 32) drained = true;
+            if (lane < ring_n) {
+                const unsigned w = base + lane;
+                const unsigned qq = kList ? mb.retrace_list[w] : w;
+                const DevScene* ssp = nullptr;
+                Vec5<double> ys;
+                double pts, pphs;
+                start_ray<kBatch>(S0, tile, B, qq, ssp, ys, pts, pphs);
+                const DevScene& Ss = kBatch ? *ssp : S0;
+                const Vec5<double> f = kerr_rhs<double>(Ss.M, Ss.a, pts, pphs, ys);
+                W.q[lane] = qq;
+                if (kBatch) W.sp[lane] = ssp;
+                W.pr[lane] = ys.pr;
+                W.pth[lane] = ys.pth;
+                W.pt[lane] = pts;
+                W.pph[lane] = pphs;
+                W.k[0][lane] = f.r;
+                W.k[1][lane] = f.th;
+                W.k[2][lane] = f.ph;
+                W.k[3][lane] = f.pr;
+                W.k[4][lane] = f.pth;
+            }
+            __syncwarp();
+        }
+        // ---- lanes without a ray take the prepared starts in order ----
+        if (need && ring_head < ring_n) {
+            const int avail = ring_n - ring_head;
+            const int rank = __popc(need & lt_mask);
+            if (!live && rank < avail) {
+                const int slot = ring_head + rank;
+                q = W.q[slot];
+                if (kBatch) sp = W.sp[slot];
+                y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], W.pr[slot], W.pth[slot]};
+                pt = W.pt[slot];
+                pph = W.pph[slot];
+                k1 = Vec5<double>{W.k[0][slot], W.k[1][slot], W.k[2][slot], W.k[3][slot], W.k[4][slot]};
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
                 ncross = 0;
                 c0 = c1 = c2 = 0.0;
-                k1_ok = false;
                 live = true;
+                ++n_rays;
             }
+            ring_head += min(__popc(need), avail);
+            __syncwarp();
         }
+        // No lane holds a ray: the queue is drained (a lane without a ray
+        // would have taken a prepared start, and a refill found none).
         if (!__any_sync(kMask, live)) break;
         int term = -1;
         if (live && retry == 0) term = start_test(S, step, y.r);
         if (live && term < 0) {
-            if (!k1_ok) {
-                k1 = kerr_rhs<double>(S.M, S.a, pt, pph, y);
-                k1_ok = true;
-            }
             Vec5<double> y5, k7;
             const double err = dp45_attempt_k1<double>(S.M, S.a, pt, pph, y, dl, k1, y5, k7);
             ++n_att;
@@ -379,12 +472,13 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
                 retry = 0;
                 ++step;
                 term = start_test(S, step, y.r);
-                // Black sky: once the escape is certain (outgoing beyond the
-                // disk, r_near and every photon orbit, far from the step
-                // budget) no crossing can follow and no star is looked up, so
-                // the colour, the crossings and the fate are those the FP64
-                // trace to r_escape would give.
-                if (term < 0 && !S.stars_on) {
+                // Re-trace on a black sky: once the escape is certain
+                // (outgoing beyond the disk, r_near and every photon orbit,
+                // far from the step budget) no crossing can follow and no star
+                // is looked up, so the colour, the crossings and the fate are
+                // those the FP64 trace to r_escape would give. (The FP64 form
+                // traces to r_escape, as the reference does.)
+                if (kList && term < 0 && !S.stars_on) {
                     const double m = kBatch ? S.mixed_margin : mb.margin;
                     const double r_near = kBatch ? S.r_near_mixed : mb.r_near;
                     const double r_min = fmax(fmax(mixed::kEscapeRMin * S.M, r_near),
@@ -396,23 +490,45 @@ mixed_retrace_kernel(const __grid_constant__ DevScene S0, const DevTile tile, co
                 ++retry;
             }
         }
-        if (live && term >= 0) {
-            live = false;
-            if (term == kTermEscaped && S.stars_on) {
-                const double b = star_brightness(S.stars, y.th, y.ph);
-                c0 += b;
-                c1 += b;
-                c2 += b;
+        // ---- finished samples: park escapes under a star sky, write the rest ----
+        const bool fin = live && term >= 0;
+        const bool star = fin && term == kTermEscaped && S.stars_on;
+        const unsigned nc = (ncross > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(ncross);
+        const unsigned fate = static_cast<unsigned>(term) | (nc << 2);
+        const unsigned smask = __ballot_sync(kMask, star);
+        if (smask) {
+            const int ns = __popc(smask);
+            if (pend_n + ns > 32) {
+                flush_star_lookups<kBatch>(W, pend_n, S0, mb);
+                pend_n = 0;
             }
-            mb.sample_rgb[3 * static_cast<size_t>(q) + 0] = c0;
-            mb.sample_rgb[3 * static_cast<size_t>(q) + 1] = c1;
-            mb.sample_rgb[3 * static_cast<size_t>(q) + 2] = c2;
-            const unsigned nc = (ncross > 0x3fffffff) ? 0x3fffffffu : static_cast<unsigned>(ncross);
-            mb.sample_fate[q] = static_cast<unsigned>(term) | (nc << 2);
+            if (star) {
+                const int slot = pend_n + __popc(smask & lt_mask);
+                W.th[slot] = y.th;
+                W.ph[slot] = y.ph;
+                W.c[0][slot] = c0;
+                W.c[1][slot] = c1;
+                W.c[2][slot] = c2;
+                W.pq[slot] = q;
+                W.pfate[slot] = fate;
+                if (kBatch) W.psp[slot] = sp;
+            }
+            pend_n += ns;
+            __syncwarp();
+        }
+        if (fin) {
+            live = false;
+            if (!star) {
+                mb.sample_rgb[3 * static_cast<size_t>(q) + 0] = c0;
+                mb.sample_rgb[3 * static_cast<size_t>(q) + 1] = c1;
+                mb.sample_rgb[3 * static_cast<size_t>(q) + 2] = c2;
+                mb.sample_fate[q] = fate;
+            }
         }
     }
 #undef S
-    warp_add(stats, n_att, n_acc, 0ull, n_att);
+    if (pend_n) flush_star_lookups<kBatch>(W, pend_n, S0, mb);
+    warp_add(stats, n_att, n_acc, kList ? 0ull : n_rays, n_att);
 }
 
 // Per pixel: sum the spp sample colours in order, scale, write the outputs.
@@ -508,19 +624,24 @@ struct MixLaunchShape {
     int sms = 0;
     int per_spec = 1, per_retrace = 1;      // resident blocks per SM, one camera
     int per_spec_b = 1, per_retrace_b = 1;  // the batch instantiations
+    int per_fp64 = 1;                       // the FP64 form's trace of every sample
 };
 const MixLaunchShape& mix_shape() {
     return per_device_shape<MixLaunchShape>([](int dev) {
         MixLaunchShape sh;
         cudaDeviceGetAttribute(&sh.sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec, mixed_speculate_kernel<false>, kMixThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, mixed_retrace_kernel<false>, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, fp64_trace_kernel<true, false>, kMixThreads,
+                                                      0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_fp64, fp64_trace_kernel<false, false>, kMixThreads, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec_b, mixed_speculate_kernel<true>, kMixThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace_b, mixed_retrace_kernel<true>, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace_b, fp64_trace_kernel<true, true>, kMixThreads,
+                                                      0);
         if (sh.per_spec < 1) sh.per_spec = 1;
         if (sh.per_retrace < 1) sh.per_retrace = 1;
         if (sh.per_spec_b < 1) sh.per_spec_b = 1;
         if (sh.per_retrace_b < 1) sh.per_retrace_b = 1;
+        if (sh.per_fp64 < 1) sh.per_fp64 = 1;
         return sh;
     });
 }
@@ -588,7 +709,8 @@ cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const D
         if (e != cudaSuccess) return e;
         m.retrace_list = ordered;
     }
-    mixed_retrace_kernel<false><<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, m, stats);
+    fp64_trace_kernel<true, false>
+        <<<sh.sms * sh.per_retrace, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, m, m.queue2, 0u, stats);
     return cudaGetLastError();
 }
 
@@ -638,6 +760,29 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
     return e;
 }
 
+cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                             const LaunchResources& res, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+    const int g2 = S.grid * S.grid;
+    const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
+    if (n == 0) return cudaSuccess;
+    // (the counter runs up to 32 items per warp past the end, and a cancel
+    // pushes it to 0x7f7f7f7f)
+    if (scratch_bytes < mixed_scratch_bytes(tile, g2) || n > 0x7f000000u) return cudaErrorInvalidValue;
+    // the work counter doubles as the progress counter (samples taken)
+    const DevMixedBuffers mb = mixed_buffers(scratch, n, res.queue);
+    cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const MixLaunchShape& sh = mix_shape();
+    const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
+    int blocks = sh.sms * sh.per_fp64;
+    if (need < blocks) blocks = need;
+    fp64_trace_kernel<false, false><<<blocks, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, mb, res.queue,
+                                                                         static_cast<unsigned>(n), res.stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_mixed_resolve(S, tile, mb, out, res.stats, stream);
+}
+
 int mixed_batch_max_blocks_per_sm() { return mix_shape().per_spec_b; }
 
 cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* out_rgba, unsigned* queue,
@@ -668,8 +813,8 @@ cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* o
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    mixed_retrace_kernel<true><<<sh.sms * per(sh.per_retrace_b), kMixThreads, 0, stream>>>(none, no_tile, B, mb,
-                                                                                            stats);
+    fp64_trace_kernel<true, true><<<sh.sms * per(sh.per_retrace_b), kMixThreads, 0, stream>>>(none, no_tile, B, mb,
+                                                                                               mb.queue2, 0u, stats);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int rb = static_cast<int>((B.n_pixels + 255) / 256);

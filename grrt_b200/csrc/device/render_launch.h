@@ -63,9 +63,15 @@ cudaError_t order_by_cost(const DevScene& S, const DevTile& tile, const unsigned
 // Doubles of spectral scratch a launch with nb bins needs on the current device.
 size_t volume_spectral_scratch_elems(int nb);
 
-// Thin-disk render, FP64 form.
+// Thin-disk render, FP64 form, one lane per pixel (thin_render.cu): the
+// diagnostic instantiation (res.diag_hamiltonian) and the batched form use it.
 cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
                         const LaunchResources& res, cudaStream_t stream);
+// Thin-disk render, FP64 form, by samples (mixed_render.cu): the FP64 trace of
+// every sample into the per-sample buffers of a mixed scratch
+// (mixed_scratch_bytes), then the resolve. The same arithmetic as launch_thin.
+cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
+                             const LaunchResources& res, void* scratch, size_t scratch_bytes, cudaStream_t stream);
 
 // Volumetric RGB render, FP64 form; and its mixed form (FP32 speculation with
 // the thin form's star pass, FP64 re-trace, resolve: scratch of
