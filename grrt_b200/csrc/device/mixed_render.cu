@@ -125,21 +125,6 @@ __device__ __forceinline__ void warp_add(DevStats* st, unsigned long long a, uns
     }
 }
 
-// Warp-aggregated fetch of the next work index; returns ~0u when exhausted.
-__device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned total) {
-    const int lane = threadIdx.x & 31;
-    const unsigned m = __ballot_sync(kMask, want);
-    unsigned base = 0;
-    if (m) {
-        const int leader = __ffs(m) - 1;
-        if (lane == leader) base = atomicAdd(counter, static_cast<unsigned>(__popc(m)));
-        base = __shfl_sync(kMask, base, leader);
-    }
-    if (!want) return ~0u;
-    const unsigned q = base + __popc(m & ((1u << lane) - 1u));
-    return q < total ? q : ~0u;
-}
-
 }  // namespace
 
 // Every kernel below comes in two instantiations: kBatch = false renders the
@@ -147,6 +132,22 @@ __device__ __forceinline__ unsigned fetch(bool want, unsigned* counter, unsigned
 // every item of the batch B (scenes in global memory, one per lane's sample),
 // over one sample space, so one launch per phase covers all cameras.
 // Inside, S names the scene of the lane's current sample.
+
+namespace {
+// Per-warp staging of the FP32 speculation's starts in shared memory (one
+// slot per lane, fields as arrays): the warp takes 32 samples at once, and
+// every lane forms one sample's camera ray, its black-sky closed-form test and
+// the FP32 first stage f(y), so that work runs with the whole warp instead of
+// one lane at a time as rays end. Samples the closed-form test settles are
+// written there and then; the rest are compacted into the slots, which lanes
+// whose ray ended take in order.
+struct SpecStage {
+    double pr[32], pth[32], pt[32], pph[32];  // start momentum (r, theta, phi are the camera's)
+    float k[5][32];                           // FP32 f(y) at the start
+    unsigned q[32];                           // sample index
+    const DevScene* sp[32];                   // batch: the sample's scene
+};
+}  // namespace
 
 // Five resident blocks per SM (at most 96 registers): the issue-bound FP32
 // pass gains more from the fifth block's warps than it loses to the few
@@ -156,6 +157,10 @@ template <bool kBatch>
 __global__ void __launch_bounds__(kMixThreads, 5)
 mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, const __grid_constant__ DevBatch B,
                        DevMixedBuffers mb, DevStats* stats) {
+    __shared__ SpecStage stage_all[kMixThreads / 32];
+    SpecStage& W = stage_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
     const DevScene* sp = nullptr;
 #define S (kBatch ? *sp : S0)
     const unsigned total = kBatch ? B.n_samples
@@ -163,63 +168,115 @@ mixed_speculate_kernel(const __grid_constant__ DevScene S0, const DevTile tile, 
                                                   : static_cast<unsigned>(tile.w) * tile.h * (S0.grid * S0.grid));
     float Mf = static_cast<float>(S0.M), af = static_cast<float>(S0.a);
     unsigned long long n_att = 0, n_acc = 0, n_rays = 0;
+    // warp-uniform: prepared slots [ring_head, ring_n) and the queue state
+    int ring_head = 0, ring_n = 0;
+    bool drained = false;
     unsigned q = ~0u;
-    bool live = false, exhausted = false;
+    bool live = false;
     Vec5<double> y;
-    Vec5<float> k1;  // FP32 f(y), kept from the previous attempt when k1_ok
-    bool k1_ok = false;
-    bool settled = false;  // black sky, never reaches the disk: final without a trace
+    Vec5<float> k1;  // FP32 f(y), kept from the previous attempt
     double pt = 0, pph = 0, dl = 0;
     int retry = 0, step = 0;
     mixed::Tracker trk;
     while (true) {
-        const bool want = !live && !exhausted;
-        const unsigned nq = fetch(want, mb.queue, total);
-        if (want) {
-            if (nq == ~0u) {
-                exhausted = true;
-            } else {
-                q = (!kBatch && mb.spec_list) ? mb.spec_list[nq] : nq;
-                start_ray<kBatch>(S0, tile, B, q, sp, y, pt, pph);
+        const unsigned need = __ballot_sync(kMask, !live);
+        // ---- the warp prepares its next starts (every lane one sample) ----
+        while (need && ring_head == ring_n && !drained) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(mb.queue, 32u);
+            base = __shfl_sync(kMask, base, 0);
+            const int n_take = base < total ? static_cast<int>(min(32u, total - base)) : 0;
+            if (n_take < 32) drained = true;
+            bool keep = false;
+            unsigned qq = 0;
+            const DevScene* ssp = nullptr;
+            Vec5<double> ys;
+            double pts = 0.0, pphs = 0.0;
+            if (lane < n_take) {
+                qq = (!kBatch && mb.spec_list) ? mb.spec_list[base + lane] : base + lane;
+                start_ray<kBatch>(S0, tile, B, qq, ssp, ys, pts, pphs);
+                const DevScene& Ss = kBatch ? *ssp : S0;
+                // Black sky: a ray whose smallest radius (closed form, from its
+                // constants of motion) lies outside the disk, r_near and every
+                // photon orbit escapes with colour 0 and no crossing.
+                bool settled = false;
+                if (!Ss.stars_on && (kBatch || !mb.spec_list)) {
+                    const double p[4] = {pts, ys.pr, ys.pth, pphs};
+                    const double m = kBatch ? Ss.mixed_margin : mb.margin;
+                    const double r_near = kBatch ? Ss.r_near_mixed : mb.r_near;
+                    const double r_gate =
+                        fmax(fmax(mixed::kEscapeRMin * Ss.M, r_near), Ss.disk_on ? Ss.r_out + 2.0 * m : 0.0);
+                    settled = surr::camera_ray_clears(Ss.M, Ss.a, Ss.r_stop - 0.01, Ss.cam_pos[1], Ss.cam_pos[2],
+                                                      p, r_gate);
+                }
+                if (settled) {
+                    const size_t o = 3 * static_cast<size_t>(qq);
+                    mb.sample_rgb[o + 0] = 0.0;
+                    mb.sample_rgb[o + 1] = 0.0;
+                    mb.sample_rgb[o + 2] = 0.0;
+                    mb.sample_fate[qq] = static_cast<unsigned>(kTermEscaped);
+                    ++n_rays;
+                } else {
+                    keep = true;
+                }
+            }
+            const unsigned km = __ballot_sync(kMask, keep);
+            if (keep) {
+                const int slot = __popc(km & lt_mask);
+                const DevScene& Ss = kBatch ? *ssp : S0;
+                const float Ms = kBatch ? static_cast<float>(Ss.M) : Mf;
+                const float as = kBatch ? static_cast<float>(Ss.a) : af;
+                const Vec5<float> f = mixed_k1(Ms, as, static_cast<float>(pts), static_cast<float>(pphs), ys);
+                W.q[slot] = qq;
+                if (kBatch) W.sp[slot] = ssp;
+                W.pr[slot] = ys.pr;
+                W.pth[slot] = ys.pth;
+                W.pt[slot] = pts;
+                W.pph[slot] = pphs;
+                W.k[0][slot] = f.r;
+                W.k[1][slot] = f.th;
+                W.k[2][slot] = f.ph;
+                W.k[3][slot] = f.pr;
+                W.k[4][slot] = f.pth;
+            }
+            ring_head = 0;
+            ring_n = __popc(km);
+            __syncwarp();
+        }
+        // ---- lanes without a ray take the prepared starts in order ----
+        if (need && ring_head < ring_n) {
+            const int avail = ring_n - ring_head;
+            const int rank = __popc(need & lt_mask);
+            if (!live && rank < avail) {
+                const int slot = ring_head + rank;
+                q = W.q[slot];
                 if (kBatch) {
+                    sp = W.sp[slot];
                     Mf = static_cast<float>(S.M);
                     af = static_cast<float>(S.a);
                 }
+                y = Vec5<double>{S.cam_pos[1], S.cam_pos[2], S.cam_pos[3], W.pr[slot], W.pth[slot]};
+                pt = W.pt[slot];
+                pph = W.pph[slot];
+                k1 = Vec5<float>{W.k[0][slot], W.k[1][slot], W.k[2][slot], W.k[3][slot], W.k[4][slot]};
                 dl = S.dl0;
                 retry = 0;
                 step = 0;
-                k1_ok = false;
                 if (kBatch)
                     trk.reset(S.disk_on, S.r_in, S.r_out, S.mixed_margin, S.r_near_mixed, S.a, pt, pph, y.th);
                 else
                     trk.reset(S.disk_on, S.r_in, S.r_out, mb.margin, mb.r_near, S.a, pt, pph, y.th);
-                // Black sky: a ray whose smallest radius (closed form, from its
-                // constants of motion) lies outside the disk, r_near and every
-                // photon orbit escapes with colour 0 and no crossing.
-                settled = false;
-                if (!S.stars_on && (kBatch || !mb.spec_list)) {
-                    const double p[4] = {pt, y.pr, y.pth, pph};
-                    const double m = kBatch ? S.mixed_margin : mb.margin;
-                    const double r_near = kBatch ? S.r_near_mixed : mb.r_near;
-                    const double r_gate =
-                        fmax(fmax(mixed::kEscapeRMin * S.M, r_near), S.disk_on ? S.r_out + 2.0 * m : 0.0);
-                    settled =
-                        surr::camera_ray_clears(S.M, S.a, S.r_stop - 0.01, S.cam_pos[1], S.cam_pos[2], p, r_gate);
-                }
                 live = true;
             }
+            ring_head += min(__popc(need), avail);
+            __syncwarp();
         }
         if (!__any_sync(kMask, live)) break;
         int term = -1;
         bool retrace = false;
         Vec5<float> k7;
         if (live && retry == 0) term = start_test(S, step, y.r);
-        if (live && term < 0 && settled) term = kTermEscaped;
         if (live && term < 0) {
-            if (!k1_ok) {
-                k1 = mixed_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y);
-                k1_ok = true;
-            }
             Vec5<double> y5;
             const double err =
                 mixed_attempt_k1(Mf, af, static_cast<float>(pt), static_cast<float>(pph), y, dl, k1, y5, k7);
