@@ -72,7 +72,7 @@ F_ATTEMPT_EXEC = 6 * F_EVAL + 480
 # operations divided by its attempts; a fused multiply-add counts 2), from the
 # ncu instruction counters of a 512x512 4-spp frame
 # (profiles/executed_flops_thin_mixed_kernels_kerr_512x512_4spp.md): the FP64
-# kernels (thin_render_kernel, mixed_retrace_kernel) and the FP32 speculation
+# kernels (fp64_trace_kernel in both forms) and the FP32 speculation
 # (packed two-wide instructions count once there: a lower bound).
 F_EXEC_FP64_ATTEMPT = 1022.8
 F_EXEC_FP32_ATTEMPT = 479.4
@@ -873,15 +873,16 @@ def main():
                            "ms_per_step": r["ms"],
                            "phase_ms": r["phase_ms"], "attempts_per_ray": st["attempts"] / my_rays,
                            "fp64_attempt_share": st["fp64_attempts"] / max(1, st["attempts"])}
-        # FP64 form: thin_render_kernel, FP64 FLOPs against the DGEMM peak
+        # FP64 form: fp64_trace_kernel (phase 0; phase 1 is the resolve), FP64
+        # FLOPs against the DGEMM peak
         st64 = res[G.FORM_FP64]["stats"]
         fl64 = st64["attempts"] * F_ATTEMPT_EXEC + my_rays * F_EVAL
         a64 = fl64 / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
-        forms["fp64"]["roofline"] = {"kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": a64,
+        forms["fp64"]["roofline"] = {"kernel": "fp64_trace_kernel<false, false>", "bound": "fp64", "achieved": a64,
                                      "peak": p64, "unit": "TFLOP/s", "frac": a64 / p64}
         e64 = st64["attempts"] * F_EXEC_FP64_ATTEMPT / (res[G.FORM_FP64]["phase_ms"][0] * 1e-3) / 1e12
         forms["fp64"]["roofline_executed"] = {
-            "kernel": "thin_render_kernel<0>", "bound": "fp64", "achieved": e64, "peak": p64, "unit": "TFLOP/s",
+            "kernel": "fp64_trace_kernel<false, false>", "bound": "fp64", "achieved": e64, "peak": p64, "unit": "TFLOP/s",
             "frac": e64 / p64, "flop_count": f"{F_EXEC_FP64_ATTEMPT} executed FP64 flop per attempt (ncu counters)"}
         # mixed form: the speculation kernel (FP32 FLOPs vs the SGEMM peak) and
         # the re-trace kernel (FP64 FLOPs vs the DGEMM peak)
@@ -890,7 +891,7 @@ def main():
         spec_att = stm["attempts"] - stm["fp64_attempts"]
         a_spec = (spec_att * F_ATTEMPT_EXEC + my_rays * F_EVAL) / (ph[0] * 1e-3) / 1e12
         a_re = stm["fp64_attempts"] * F_ATTEMPT_EXEC / (ph[2] * 1e-3) / 1e12
-        forms["mixed"]["phases"] = ["mixed_speculate_kernel", "mixed_star_kernel", "mixed_retrace_kernel",
+        forms["mixed"]["phases"] = ["mixed_speculate_kernel", "mixed_star_kernel", "fp64_trace_kernel<true, false>",
                                     "mixed_resolve_kernel"]
         forms["mixed"]["roofline"] = {
             "speculate": {"bound": "fp32", "achieved": a_spec, "peak": p32, "unit": "TFLOP/s", "frac": a_spec / p32},

@@ -401,11 +401,11 @@ int GRRTContext::render_rgb_device(const DevTile& tile, float* d_rgba, double* d
         e = launch_thin_mixed(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, mixed_margin,
                               mixed_r_near(), ev_phase, s);
     else if (fp64_thin)
-        e = launch_thin_fp64(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, s);
+        e = launch_thin_fp64(S, tile, out, res, d_mixed_scratch, d_mixed_scratch_bytes, ev_phase, s);
     else
         e = launch_thin(S, tile, out, res, s);
     cudaEventRecord(ev1, s);
-    n_phases = (mixed_thin || mixed_vol) ? kMixedPhases : 0;
+    n_phases = (mixed_thin || mixed_vol) ? kMixedPhases : fp64_thin ? kFp64Phases : 0;
     if (fail_cuda(e, "render launch")) return -1;
     return 0;
 }

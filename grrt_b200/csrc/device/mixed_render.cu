@@ -818,7 +818,11 @@ cudaError_t launch_thin_mixed(const DevScene& S, const DevTile& tile, const Thin
 }
 
 cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                             const LaunchResources& res, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+                             const LaunchResources& res, void* scratch, size_t scratch_bytes,
+                             cudaEvent_t* phase_events, cudaStream_t stream) {
+    auto mark = [&](int k) {
+        if (phase_events) cudaEventRecord(phase_events[k], stream);
+    };
     const int g2 = S.grid * S.grid;
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
     if (n == 0) return cudaSuccess;
@@ -833,11 +837,15 @@ cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinO
     const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
     int blocks = sh.sms * sh.per_fp64;
     if (need < blocks) blocks = need;
+    mark(0);
     fp64_trace_kernel<false, false><<<blocks, kMixThreads, 0, stream>>>(S, tile, DevBatch{}, mb, res.queue,
                                                                          static_cast<unsigned>(n), res.stats);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    return launch_mixed_resolve(S, tile, mb, out, res.stats, stream);
+    mark(1);
+    e = launch_mixed_resolve(S, tile, mb, out, res.stats, stream);
+    mark(2);
+    return e;
 }
 
 int mixed_batch_max_blocks_per_sm() { return mix_shape().per_spec_b; }

@@ -70,8 +70,11 @@ cudaError_t launch_thin(const DevScene& S, const DevTile& tile, const ThinOutput
 // Thin-disk render, FP64 form, by samples (mixed_render.cu): the FP64 trace of
 // every sample into the per-sample buffers of a mixed scratch
 // (mixed_scratch_bytes), then the resolve. The same arithmetic as launch_thin.
+// phase_events: NULL, or kFp64Phases + 1 events (trace, resolve).
+constexpr int kFp64Phases = 2;
 cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinOutputs& out,
-                             const LaunchResources& res, void* scratch, size_t scratch_bytes, cudaStream_t stream);
+                             const LaunchResources& res, void* scratch, size_t scratch_bytes,
+                             cudaEvent_t* phase_events, cudaStream_t stream);
 
 // Volumetric RGB render, FP64 form; and its mixed form (FP32 speculation with
 // the thin form's star pass, FP64 re-trace, resolve: scratch of

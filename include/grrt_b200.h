@@ -79,8 +79,10 @@ GRRT_EXPORT int grrt_set_mixed_params(GRRTContext* ctx, double r_factor, double 
 
 /* Device time (ms, CUDA events on the render stream) of each kernel phase of
  * the last render: the mixed thin-disk form has 4 (FP32 speculation, star
- * pass, FP64 re-trace, resolve); every other render has 1. Writes at most
- * capacity values; returns the number of phases, or -1. Waits for the render. */
+ * pass, FP64 re-trace, resolve), the thin-disk FP64 form 2 (FP64 trace,
+ * resolve), the volumetric mixed forms 3 (FP32 speculation, FP64 re-trace,
+ * resolve); every other render has 1. Writes at most capacity values; returns
+ * the number of phases, or -1. Waits for the render. */
 GRRT_EXPORT int grrt_get_phase_ms(GRRTContext* ctx, double* out, int capacity);
 
 /* RGB render into device memory (the loop of Renderer::render,
