@@ -444,6 +444,7 @@ class Batch:
 
     ORDER_CAMERA_MAJOR = 0
     ORDER_ROUND_ROBIN = 1
+    ORDER_SAMPLES = 2  # FP64 thin-disk batches: traced by samples (chunk size and block size do not apply)
 
     def __init__(self, cameras: Sequence[dict], freqs: Optional[Sequence] = None):
         """freqs: per camera, the bins (Hz) of a volumetric camera or None. As

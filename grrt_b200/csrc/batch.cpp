@@ -73,6 +73,7 @@ struct GRRTBatch {
     cudaGraphExec_t graph = nullptr;
     void* graph_out = nullptr;
     int graph_form = -1, graph_blocks = -1, graph_block = -1;
+    bool graph_samples = false;
     bool schedule_dirty = true;
     std::string error;
 
@@ -110,7 +111,7 @@ struct GRRTBatch {
                 per[it].push_back(DevBatchChunk{static_cast<int>(it), s, std::min(chunk_size, n - s)});
         }
         std::vector<DevBatchChunk> out;
-        if (order == GRRT_BATCH_ORDER_CAMERA_MAJOR) {
+        if (order != GRRT_BATCH_ORDER_ROUND_ROBIN) {
             for (auto& v : per) out.insert(out.end(), v.begin(), v.end());
         } else {
             size_t longest = 0;
@@ -156,8 +157,12 @@ struct GRRTBatch {
         return B;
     }
 
+    // FP64 thin-disk batch traced by samples (GRRT_BATCH_ORDER_SAMPLES)
+    bool by_samples() const { return !spectral && form != GRRT_FORM_MIXED && order == GRRT_BATCH_ORDER_SAMPLES; }
+
     int max_blocks_per_sm() const {
         if (spectral) return vol_spectral_batch_max_blocks_per_sm();
+        if (by_samples()) return fp64_batch_max_blocks_per_sm();
         return form == GRRT_FORM_MIXED ? mixed_batch_max_blocks_per_sm() : thin_batch_max_blocks_per_sm(block);
     }
 
@@ -190,6 +195,7 @@ struct GRRTBatch {
         if (!upload_schedule()) return -1;
         const int nb = blocks();
         const bool mixed = !spectral && form == GRRT_FORM_MIXED;
+        const bool samples = by_samples();
         if (spectral) {
             const size_t need = static_cast<size_t>(4) * nb_max * nb * vol_spectral_batch_threads();
             if (need > spec_scratch_elems) {
@@ -202,9 +208,10 @@ struct GRRTBatch {
                 spec_scratch_elems = need;
             }
         }
-        if (mixed) {
-            if (total_samples > 0xffffffffull) {
-                error = "the mixed form indexes samples in 32 bits; this batch has " + std::to_string(total_samples);
+        if (mixed || samples) {
+            if (total_samples > 0x7f000000ull) {
+                error = "the mixed form and the trace by samples index samples in 31 bits; this batch has " +
+                        std::to_string(total_samples);
                 return -1;
             }
             const size_t need = mixed_scratch_bytes_for(total_samples);
@@ -218,7 +225,8 @@ struct GRRTBatch {
                 mixed_bytes = need;
             }
         }
-        if (!graph || graph_out != out || graph_form != form || graph_blocks != nb || graph_block != block) {
+        if (!graph || graph_out != out || graph_form != form || graph_blocks != nb || graph_block != block ||
+            graph_samples != samples) {
             if (graph) cudaGraphExecDestroy(graph);
             graph = nullptr;
             cudaGraph_t g = nullptr;
@@ -229,7 +237,9 @@ struct GRRTBatch {
                                                      spec_scratch_elems, d_queue, d_stats, nb, stream)
                 : mixed ? launch_thin_mixed_batch(desc(), any_stars, static_cast<float4*>(out), d_queue, d_stats,
                                                   d_mixed, mixed_bytes, blocks_per_sm, stream)
-                        : launch_thin_batch(desc(), static_cast<float4*>(out), d_queue, d_stats, nb, block, stream);
+                : samples ? launch_thin_fp64_batch(desc(), static_cast<float4*>(out), d_queue, d_stats, d_mixed,
+                                                   mixed_bytes, blocks_per_sm, stream)
+                          : launch_thin_batch(desc(), static_cast<float4*>(out), d_queue, d_stats, nb, block, stream);
             const cudaError_t ce = cudaStreamEndCapture(stream, &g);
             if (fail(le, "batch launch") || fail(ce, "end capture")) {
                 if (g) cudaGraphDestroy(g);
@@ -242,6 +252,7 @@ struct GRRTBatch {
             graph_form = form;
             graph_blocks = nb;
             graph_block = block;
+            graph_samples = samples;
         }
         cudaEventRecord(ev0, s);
         if (fail(cudaGraphLaunch(graph, s), "graph launch")) return -1;
@@ -445,7 +456,9 @@ extern "C" GRRT_EXPORT int grrt_batch_get_tuning(const GRRTBatch* b, int* block,
 }
 
 extern "C" GRRT_EXPORT int grrt_batch_set_schedule(GRRTBatch* b, int chunk_size, int order, int blocks_per_sm) {
-    if (!b || chunk_size < 1 || (order != GRRT_BATCH_ORDER_CAMERA_MAJOR && order != GRRT_BATCH_ORDER_ROUND_ROBIN) ||
+    if (!b || chunk_size < 1 ||
+        (order != GRRT_BATCH_ORDER_CAMERA_MAJOR && order != GRRT_BATCH_ORDER_ROUND_ROBIN &&
+         order != GRRT_BATCH_ORDER_SAMPLES) ||
         blocks_per_sm < 0) {
         if (b) b->error = "grrt_batch_set_schedule: bad schedule";
         return -1;
@@ -591,7 +604,8 @@ extern "C" GRRT_EXPORT int grrt_batch_get_stats(GRRTBatch* b, GRRTStats* out) {
 // Times candidate schedules on the batch itself and keeps the fastest.
 //   FP64 thin-disk batches: chunk size (64..4096) x chunk order x resident
 //     blocks per SM at 128 threads per block, then threads per block (64,
-//     128, 256) x resident blocks per SM at the best chunk and order.
+//     128, 256) x resident blocks per SM at the best chunk and order; and the
+//     trace by samples (GRRT_BATCH_ORDER_SAMPLES) x resident blocks per SM.
 //   Spectral batches: chunk size x chunk order x resident blocks per SM.
 //   Mixed batches (the phases take samples in camera order, so the chunk
 //     table does not apply): resident blocks per SM x the FP32 tolerance
@@ -754,6 +768,7 @@ extern "C" GRRT_EXPORT int grrt_batch_autotune(GRRTBatch* b, const char* cache_p
             const Tuning base = best_t;
             for (int blk : {64, 256}) {
                 b->block = blk;
+                b->order = base.order;
                 const int mb = b->max_blocks_per_sm();
                 for (int bp : {mb, std::max(1, mb - 1)}) {
                     Tuning t = base;
@@ -761,6 +776,17 @@ extern "C" GRRT_EXPORT int grrt_batch_autotune(GRRTBatch* b, const char* cache_p
                     t.bps = bp;
                     if (consider(t) != 0) return -1;
                 }
+            }
+            // the trace by samples (its own kernel: 128 threads, no chunks)
+            b->block = 128;
+            b->order = GRRT_BATCH_ORDER_SAMPLES;
+            const int mbs = b->max_blocks_per_sm();
+            for (int bp : {mbs, std::max(1, mbs - 1)}) {
+                Tuning t = base;
+                t.order = GRRT_BATCH_ORDER_SAMPLES;
+                t.block = 128;
+                t.bps = bp;
+                if (consider(t) != 0) return -1;
             }
         }
     }

@@ -681,7 +681,7 @@ struct MixLaunchShape {
     int sms = 0;
     int per_spec = 1, per_retrace = 1;      // resident blocks per SM, one camera
     int per_spec_b = 1, per_retrace_b = 1;  // the batch instantiations
-    int per_fp64 = 1;                       // the FP64 form's trace of every sample
+    int per_fp64 = 1, per_fp64_b = 1;       // the FP64 form's trace of every sample (one camera, batch)
 };
 const MixLaunchShape& mix_shape() {
     return per_device_shape<MixLaunchShape>([](int dev) {
@@ -691,6 +691,8 @@ const MixLaunchShape& mix_shape() {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace, fp64_trace_kernel<true, false>, kMixThreads,
                                                       0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_fp64, fp64_trace_kernel<false, false>, kMixThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_fp64_b, fp64_trace_kernel<false, true>, kMixThreads,
+                                                      0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_spec_b, mixed_speculate_kernel<true>, kMixThreads, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh.per_retrace_b, fp64_trace_kernel<true, true>, kMixThreads,
                                                       0);
@@ -699,6 +701,7 @@ const MixLaunchShape& mix_shape() {
         if (sh.per_spec_b < 1) sh.per_spec_b = 1;
         if (sh.per_retrace_b < 1) sh.per_retrace_b = 1;
         if (sh.per_fp64 < 1) sh.per_fp64 = 1;
+        if (sh.per_fp64_b < 1) sh.per_fp64_b = 1;
         return sh;
     });
 }
@@ -849,6 +852,34 @@ cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinO
 }
 
 int mixed_batch_max_blocks_per_sm() { return mix_shape().per_spec_b; }
+
+int fp64_batch_max_blocks_per_sm() { return mix_shape().per_fp64_b; }
+
+cudaError_t launch_thin_fp64_batch(const DevBatch& B, float4* out_rgba, unsigned* queue, DevStats* stats,
+                                   void* scratch, size_t scratch_bytes, int blocks_per_sm, cudaStream_t stream) {
+    const size_t n = B.n_samples;
+    if (n == 0) return cudaSuccess;
+    if (B.n_items < 1 || scratch_bytes < mixed_scratch_bytes_for(n) || n > 0x7f000000u) return cudaErrorInvalidValue;
+    const DevMixedBuffers mb = mixed_buffers(scratch, n, queue);
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const MixLaunchShape& sh = mix_shape();
+    const int per = (blocks_per_sm > 0 && blocks_per_sm < sh.per_fp64_b) ? blocks_per_sm : sh.per_fp64_b;
+    const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
+    int blocks = sh.sms * per;
+    if (need < blocks) blocks = need;
+    const DevScene none{};
+    const DevTile no_tile{};
+    fp64_trace_kernel<false, true>
+        <<<blocks, kMixThreads, 0, stream>>>(none, no_tile, B, mb, queue, static_cast<unsigned>(n), stats);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int rb = static_cast<int>((B.n_pixels + 255) / 256);
+    if (rb > sh.sms * 8) rb = sh.sms * 8;
+    if (rb < 1) rb = 1;
+    mixed_resolve_kernel<true><<<rb, 256, 0, stream>>>(none, no_tile, B, mb, out_rgba, nullptr, nullptr, stats);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* out_rgba, unsigned* queue,
                                     DevStats* stats, void* scratch, size_t scratch_bytes, int blocks_per_sm,

@@ -186,6 +186,12 @@ cudaError_t launch_thin_mixed_batch(const DevBatch& B, bool any_stars, float4* o
                                     DevStats* stats, void* scratch, size_t scratch_bytes, int blocks_per_sm,
                                     cudaStream_t stream);
 int mixed_batch_max_blocks_per_sm();
+// Batched FP64 form by samples: the trace of launch_thin_fp64 over the
+// samples of every item in item order, then the resolve (scratch and items as
+// for launch_thin_mixed_batch).
+cudaError_t launch_thin_fp64_batch(const DevBatch& B, float4* out_rgba, unsigned* queue, DevStats* stats,
+                                   void* scratch, size_t scratch_bytes, int blocks_per_sm, cudaStream_t stream);
+int fp64_batch_max_blocks_per_sm();
 
 // Batched volumetric spectral render over many cameras, FP64 form: one
 // persistent launch of the warp-cooperative spectral kernel over the batch's

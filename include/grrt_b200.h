@@ -163,9 +163,14 @@ GRRT_EXPORT int grrt_render_spectral_device_noalloc(GRRTContext* ctx, const doub
 typedef struct GRRTBatch GRRTBatch;
 
 /* Chunk orders of the schedule: all chunks of camera 0, then camera 1, ...;
- * or chunk k of every camera before chunk k+1. */
+ * or chunk k of every camera before chunk k+1. GRRT_BATCH_ORDER_SAMPLES (FP64
+ * thin-disk batches): every camera's samples in camera order, traced by
+ * samples with the warp staging of the single FP64 render, then resolved into
+ * pixels; the chunk size and the threads per block do not apply (other
+ * batches take it as camera-major). */
 #define GRRT_BATCH_ORDER_CAMERA_MAJOR 0
 #define GRRT_BATCH_ORDER_ROUND_ROBIN 1
+#define GRRT_BATCH_ORDER_SAMPLES 2
 
 /* params: count cameras. NULL on failure with the reason in grrt_batch_error(NULL). */
 GRRT_EXPORT GRRTBatch* grrt_batch_create(const GRRTParams* params, int count);

@@ -31,12 +31,14 @@ def test_batch_equals_single_camera_renders(grrt, need_gpu):
     cams[3] = dict(cams[3], samples_per_pixel=4, width=40, height=32)  # uneven sizes and spp
     want = single_renders(grrt, cams)
     B = grrt.Batch(cams)
-    for order in (B.ORDER_ROUND_ROBIN, B.ORDER_CAMERA_MAJOR):
-        for chunk in (1, 37, 256, 100000):
-            B.set_schedule(chunk, order, 0)
-            got = B.render()
-            for k, (g, w) in enumerate(zip(got, want)):
-                np.testing.assert_array_equal(g, w, err_msg=f"camera {k}, chunk {chunk}, order {order}")
+    schedules = [(chunk, order) for order in (B.ORDER_ROUND_ROBIN, B.ORDER_CAMERA_MAJOR)
+                 for chunk in (1, 37, 256, 100000)]
+    schedules.append((256, B.ORDER_SAMPLES))  # traced by samples: the chunk size does not apply
+    for chunk, order in schedules:
+        B.set_schedule(chunk, order, 0)
+        got = B.render()
+        for k, (g, w) in enumerate(zip(got, want)):
+            np.testing.assert_array_equal(g, w, err_msg=f"camera {k}, chunk {chunk}, order {order}")
     st = B.stats()
     assert st["rays"] == sum(c["width"] * c["height"] * (4 if c["samples_per_pixel"] == 4 else 1) for c in cams)
 
