@@ -134,8 +134,10 @@ vol_spectral_kernel(const __grid_constant__ DevScene S0, const DevTile tile, con
                             fresh_pixel = true;
                         }  // else: padding slot of a short chunk, fetch again
                     } else {
-                        // list: the listed samples (kList), or the pixel order
-                        pix = static_cast<int>(list ? list[k] : k);
+                        // list: the listed samples (kList), or the pixel order;
+                        // taken in the spread order (vol_spread_order)
+                        const unsigned ks = vol_spread_order(k, total);
+                        pix = static_cast<int>(list ? list[ks] : ks);
                         smp = 0;
                         fresh_pixel = true;
                     }

@@ -14,6 +14,25 @@ struct VolCounters {
     unsigned long long clamp = 0, march = 0, physics = 0, bins = 0, fp64 = 0;
 };
 
+// Order in which the spectral kernel takes its work items: within each full
+// block of kVolSpread^2 items the order is transposed, so the 32 items a warp
+// takes at once lie kVolSpread items apart in the image. Neighbouring pixels
+// trace alike, and the costliest rays (near the photon orbit, grazing the
+// volume for thousands of clamped steps) come in clusters; a cluster taken by
+// one warp serves its lanes' physics steps one after another, while spread
+// over different warps the long rays run side by side. Items past the last
+// full block keep their index. A bijection on [0, total).
+#ifndef GRRT_VOL_SPREAD
+#define GRRT_VOL_SPREAD 64
+#endif
+constexpr unsigned kVolSpread = GRRT_VOL_SPREAD;
+__host__ __device__ __forceinline__ unsigned vol_spread_order(unsigned k, unsigned total) {
+    constexpr unsigned kBlock = kVolSpread * kVolSpread;
+    if (k >= (total / kBlock) * kBlock) return k;
+    const unsigned base = k - k % kBlock, j = k % kBlock;
+    return base + (j % kVolSpread) * kVolSpread + j / kVolSpread;
+}
+
 // Warp sum of the counters, one atomic per counter per warp.
 __device__ __forceinline__ void flush_vol(DevStats* st, const VolCounters& c, bool cancelled) {
     unsigned long long v[11] = {c.attempts, c.accepted, c.rays, c.horizon, c.escaped, c.maxsteps,
