@@ -364,7 +364,6 @@ def time_form(torch, R, form, stream, flush, render, steps, warmup, dist):
     for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    st = R.stats()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     phases = []
     if dist:
@@ -376,6 +375,7 @@ def time_form(torch, R, form, stream, flush, render, steps, warmup, dist):
         phases.append(R.phase_ms())  # waits for this frame; the next frame is enqueued after
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
+    st = R.stats()  # the last timed frame's work counters (every frame does the same work)
     if dist:
         dist.barrier()
     kernel_ms = [a.elapsed_time(b) for a, b in evs]
