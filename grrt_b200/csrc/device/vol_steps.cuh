@@ -5,6 +5,7 @@
 #pragma once
 
 #include "integrate.cuh"
+#include "shading.cuh"
 #include "volume.cuh"
 
 namespace grrt_b200 {

@@ -3,6 +3,7 @@
 #include "../../grrt_b200/csrc/device/integrate.cuh"
 #include "../../grrt_b200/csrc/device/mixed_spec.cuh"
 #include "../../grrt_b200/csrc/device/surrogate_geom.cuh"
+#include "../../grrt_b200/csrc/device/vol_steps.cuh"
 
 using namespace grrt_b200;
 
@@ -249,4 +250,11 @@ void devmath_trace_crossings(const double* sc, const double* y8, double* out) {
     out[4] = step;
     out[5] = n_extra;
 }
+
+// The spectral kernel's work order: out[k] = the item taken k-th, k < total.
+void devmath_vol_spread_order(unsigned total, unsigned* out) {
+    for (unsigned k = 0; k < total; ++k) out[k] = vol_spread_order(k, total);
+}
+
+unsigned devmath_vol_spread() { return kVolSpread; }
 }

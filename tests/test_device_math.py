@@ -19,7 +19,7 @@ OUT = os.path.join(ROOT, "_build", "test", "libdevmath.so")
 
 @pytest.fixture(scope="module")
 def devmath():
-    hdrs = [os.path.join(ROOT, "grrt_b200", "csrc", "device", f) for f in ("kerr.cuh", "integrate.cuh", "mixed_spec.cuh", "scene.h", "surrogate_geom.cuh")]
+    hdrs = [os.path.join(ROOT, "grrt_b200", "csrc", "device", f) for f in ("kerr.cuh", "integrate.cuh", "mixed_spec.cuh", "scene.h", "surrogate_geom.cuh", "vol_steps.cuh", "shading.cuh", "volume.cuh")]
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(p) for p in hdrs + [SRC]):
         os.makedirs(os.path.dirname(OUT), exist_ok=True)
         subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O2", "-shared", "-Xcompiler", "-fPIC",
@@ -121,3 +121,22 @@ def test_k1_reuse_traces_identically(grrt, oracle_lib, devmath, f32):
         np.testing.assert_array_equal(kept, fresh)
         n_rejects += int(fresh[2] - fresh[1])
     assert n_rejects > 0  # the reject path was exercised
+
+
+def test_vol_spread_order_is_a_permutation(devmath):
+    """The spectral kernel takes its work items in a spread order: every item
+    exactly once, the 32 items a warp takes together kVolSpread apart inside a
+    full block, and the items past the last full block in their own order."""
+    devmath.devmath_vol_spread.restype = C.c_uint
+    S = devmath.devmath_vol_spread()
+    B = S * S
+    for total in (0, 1, 31, B - 1, B, B + 1, 3 * B + 17, 262144, 262144 + 5):
+        out = np.zeros(max(total, 1), dtype=np.uint32)
+        devmath.devmath_vol_spread_order(C.c_uint(total), out.ctypes.data_as(C.POINTER(C.c_uint)))
+        got = out[:total].astype(np.int64)
+        assert np.array_equal(np.sort(got), np.arange(total)), total
+        full = (total // B) * B
+        if full:
+            np.testing.assert_array_equal(got[:32], np.arange(32) * S)
+            assert np.all(np.diff(got[:S]) == S)
+        np.testing.assert_array_equal(got[full:], np.arange(full, total))
