@@ -41,6 +41,9 @@ namespace {
 
 constexpr int kMixThreads = 128;
 constexpr unsigned kMask = 0xffffffffu;
+// Most samples one launch takes: the work counters run up to 32 items per
+// warp past the end, and a cancel pushes them to 0x7f7f7f7f.
+constexpr size_t kMaxSamples = 0x7f000000u;
 
 __device__ __forceinline__ void sample_start(const DevScene& S, const DevTile& tile, unsigned q, int g2,
                                              Vec5<double>& y, double& pt, double& pph) {
@@ -730,6 +733,9 @@ cudaError_t launch_mixed_speculate(const DevScene& S, const DevTile& tile, const
                                    DevStats* stats, cudaStream_t stream) {
     const MixLaunchShape& sh = mix_shape();
     const size_t n = static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid;
+    // the work counters run up to 32 items per warp past the end, and a cancel
+    // pushes them to 0x7f7f7f7f
+    if (n > kMaxSamples) return cudaErrorInvalidValue;
     const int need = static_cast<int>((n + kMixThreads - 1) / kMixThreads);
     mixed_speculate_kernel<false>
         <<<need < sh.sms * sh.per_spec ? need : sh.sms * sh.per_spec, kMixThreads, 0, stream>>>(S, tile, DevBatch{},
@@ -751,6 +757,7 @@ cudaError_t launch_mixed_stars(const DevScene& S, const DevTile& tile, const Dev
 cudaError_t launch_mixed_retrace(const DevScene& S, const DevTile& tile, const DevMixedBuffers& mb, DevStats* stats,
                                  void* scratch, cudaStream_t stream) {
     const MixLaunchShape& sh = mix_shape();
+    if (static_cast<size_t>(tile.w) * tile.h * S.grid * S.grid > kMaxSamples) return cudaErrorInvalidValue;
     DevMixedBuffers m = mb;
     if (!S.stars_on) {
         // Black sky: the list holds lit samples near the hole, whose lengths
@@ -829,9 +836,7 @@ cudaError_t launch_thin_fp64(const DevScene& S, const DevTile& tile, const ThinO
     const int g2 = S.grid * S.grid;
     const size_t n = static_cast<size_t>(tile.w) * tile.h * g2;
     if (n == 0) return cudaSuccess;
-    // (the counter runs up to 32 items per warp past the end, and a cancel
-    // pushes it to 0x7f7f7f7f)
-    if (scratch_bytes < mixed_scratch_bytes(tile, g2) || n > 0x7f000000u) return cudaErrorInvalidValue;
+    if (scratch_bytes < mixed_scratch_bytes(tile, g2) || n > kMaxSamples) return cudaErrorInvalidValue;
     // the work counter doubles as the progress counter (samples taken)
     const DevMixedBuffers mb = mixed_buffers(scratch, n, res.queue);
     cudaError_t e = cudaMemsetAsync(res.queue, 0, sizeof(unsigned), stream);
@@ -859,7 +864,7 @@ cudaError_t launch_thin_fp64_batch(const DevBatch& B, float4* out_rgba, unsigned
                                    void* scratch, size_t scratch_bytes, int blocks_per_sm, cudaStream_t stream) {
     const size_t n = B.n_samples;
     if (n == 0) return cudaSuccess;
-    if (B.n_items < 1 || scratch_bytes < mixed_scratch_bytes_for(n) || n > 0x7f000000u) return cudaErrorInvalidValue;
+    if (B.n_items < 1 || scratch_bytes < mixed_scratch_bytes_for(n) || n > kMaxSamples) return cudaErrorInvalidValue;
     const DevMixedBuffers mb = mixed_buffers(scratch, n, queue);
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
