@@ -2,8 +2,11 @@
 // emission summed over every equatorial crossing inside [r_in, r_out] ->
 // first-match star lookup on escape. The per-pixel path of
 // GeodesicTracer::trace (src/geodesic_tracer.cpp:23-181) inside the loop of
-// Renderer::render (src/renderer.cpp:30-82), in the FP64 form (the mixed form
-// of the thin disk is mixed_render.cu).
+// Renderer::render (src/renderer.cpp:30-82), in the FP64 form, one lane per
+// pixel. This kernel serves the Hamiltonian diagnostic (GRRT_DIAG_HAMILTONIAN)
+// and the batched form's pixel schedules; the FP64 form's renders otherwise
+// trace by samples with the per-sample work staged per warp
+// (fp64_trace_kernel in mixed_render.cu, the same arithmetic).
 //
 // Execution model: a persistent grid (resident blocks only). Each lane owns one
 // pixel at a time and walks its spp samples; each loop iteration performs
