@@ -29,7 +29,9 @@ on its stream; a 256 MiB buffer is written between steps to flush the 126 MB
 L2). Both forms are timed; "forms" reports each, with per-kernel phase times
 from the library's own CUDA events. `e2e` is the same metric through the
 reference C entry point grrt_render with a host framebuffer (launch
-parameters in, the float RGBA frame out, every step).
+parameters in, the float RGBA frame out, every step): a page-locked buffer,
+which the library copies into directly, and, under e2e.pageable, a pageable
+one, which it fills through its pinned staging buffer.
 """
 from __future__ import annotations
 
@@ -827,39 +829,50 @@ def main():
     # end to end, headline form: whole frames through the reference C entry
     # point (host framebuffer); with rows sharded, each rank's rows, the
     # all-gather and rank 0's copy of the frame to the host
-    host_fb = np.empty((H, W, 4), dtype=np.float32)
+    # The framebuffer is page-locked host memory (the library copies into it
+    # directly); the same call into pageable memory (numpy) is timed beside it.
     import ctypes as C
     L = G.lib()
-    fbp = host_fb.ctypes.data_as(C.POINTER(C.c_float))
+    host_pinned = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    host_pageable = np.empty((H, W, 4), dtype=np.float32)
 
-    def e2e_frame():
+    def e2e_frame(fb_t, fbp):
         if rows:
             with torch.cuda.stream(stream):
                 frame = render()
             stream.synchronize()
             if rank == 0:
-                host_fb[...] = frame.cpu().numpy()
+                fb_t.copy_(frame.reshape(fb_t.shape))
         else:
             rc = L.grrt_render(R.ctx, fbp)
             assert rc == 0, L.grrt_error(R.ctx)
-    for _ in range(2):
-        e2e_frame()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = time.perf_counter()
-    e2e_steps = max(3, args.steps // 2)
-    for _ in range(e2e_steps):
-        e2e_frame()
-    e2e_s = (time.perf_counter() - e0) / e2e_steps
-    if dist:
-        e2e_s = G.multi.max_over_ranks(e2e_s, dist, "cuda")
+
+    def e2e_time(fb_t, fbp):
+        for _ in range(2):
+            e2e_frame(fb_t, fbp)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = time.perf_counter()
+        n_e2e = max(3, args.steps // 2)
+        for _ in range(n_e2e):
+            e2e_frame(fb_t, fbp)
+        t = (time.perf_counter() - e0) / n_e2e
+        if dist:
+            t = G.multi.max_over_ranks(t, dist, "cuda")
+        return t
+
+    e2e_s = e2e_time(host_pinned, C.cast(host_pinned.data_ptr(), C.POINTER(C.c_float)))
+    e2e_pageable_s = e2e_time(torch.from_numpy(host_pageable),
+                              host_pageable.ctypes.data_as(C.POINTER(C.c_float)))
     e2e = {"value": frames_per_step * RAYS / e2e_s, "unit": "rays/s",
            "h2d_bytes_per_step": 1536,  # launch parameters (scene description) per frame
            "d2h_bytes_per_step": W * H * 16,  # float RGBA frame
            "api": ("grrt_render_rows_device + all-gather + copy to host" if rows
                    else "grrt_render(ctx, float* host_framebuffer)"),
-           "form": args.form, "ms_per_step": 1e3 * e2e_s}
+           "host_buffer": "page-locked (pinned)",
+           "form": args.form, "ms_per_step": 1e3 * e2e_s,
+           "pageable": {"value": frames_per_step * RAYS / e2e_pageable_s, "ms_per_step": 1e3 * e2e_pageable_s}}
 
     if rank == 0:
         peaks = measured_peaks(torch)

@@ -490,12 +490,21 @@ bool GRRTContext::stage_pinned(size_t bytes) {
     return h_stage != nullptr;
 }
 
-// Device-to-host copy of a finished result into caller memory (pageable, as a
-// caller's framebuffer usually is): through a pinned staging buffer in
-// kCopyChunks chunks, each chunk's copy into the caller's buffer spread over
-// the host threads while the next chunks cross the bus. Falls back to one
-// plain copy for small results or when no pinned memory can be had.
+// Device-to-host copy of a finished result into caller memory. Page-locked
+// caller memory (cudaMallocHost, cudaHostRegister) takes one direct copy.
+// Pageable memory, as a caller's framebuffer usually is, goes through a pinned
+// staging buffer in kCopyChunks chunks, each chunk's copy into the caller's
+// buffer spread over the host threads while the next chunks cross the bus;
+// small results, or no pinned memory to be had, take one plain copy.
 int GRRTContext::copy_to_host(void* host, const void* d, size_t bytes, cudaStream_t s) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, host) == cudaSuccess && attr.type == cudaMemoryTypeHost) {
+        if (fail_cuda(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, s), "copy result") ||
+            fail_cuda(cudaStreamSynchronize(s), "copy result"))
+            return -1;
+        return 0;
+    }
+    cudaGetLastError();
     constexpr size_t kMin = size_t(4) << 20;
     const bool events = bytes >= kMin && stage_pinned(bytes);
     if (!events) return fail_cuda(cudaMemcpy(host, d, bytes, cudaMemcpyDeviceToHost), "copy result") ? -1 : 0;

@@ -35,3 +35,25 @@ def test_host_spectral_render_equals_device_render(grrt, need_gpu):
     want = dev.cpu().numpy()
     got = R.render_spectral()
     np.testing.assert_array_equal(got.reshape(want.shape), want)
+
+
+def test_host_render_into_page_locked_buffer(grrt, need_gpu):
+    """A page-locked framebuffer (here torch's pinned memory) takes one direct
+    copy instead of the staging path; the caller still gets exactly the
+    device result."""
+    import ctypes as C
+    import torch
+    w, h = 601, 499
+    R = grrt.Renderer(grrt.config_params(2, width=w, height=h, spp=1))
+    R.set_precision(grrt.FORM_MIXED)
+    dev = torch.full((h, w, 4), float("nan"), dtype=torch.float32, device="cuda")
+    R.render_device(dev)
+    torch.cuda.synchronize()
+    want = dev.cpu().numpy()
+    fb = torch.full((h, w, 4), float("nan"), dtype=torch.float32).pin_memory()
+    L = grrt.lib()
+    for _ in range(2):
+        fb.fill_(float("nan"))
+        rc = L.grrt_render(R.ctx, C.cast(fb.data_ptr(), C.POINTER(C.c_float)))
+        assert rc == 0, L.grrt_error(R.ctx)
+        np.testing.assert_array_equal(fb.numpy(), want)
