@@ -112,6 +112,26 @@ def test_fits_repeated_and_larger_than_one_copy_group(grrt, need_gpu, tmp_path):
     assert (host > 0).any()
 
 
+def test_fits_cube_of_several_megabytes(grrt, need_gpu, tmp_path):
+    """A cube of a few megabytes in several copy groups (odd sizes): the file
+    has the FITS layout (header, data, zero padding to a whole number of
+    2880-byte blocks) and holds the host render bit for bit, on repeated
+    calls into fresh files."""
+    W, H, nb = 97, 61, 33  # 1.56 MB of data
+    freqs = grrt.log_bins(1e14, 1e18, nb)
+    R = grrt.Renderer(grrt.config_params(3, width=W, height=H), freqs=freqs)
+    host = R.render_spectral()
+    for name in ("a.fits", "b.fits"):
+        path = str(tmp_path / name)
+        R.render_fits(path, W, H)
+        raw = open(path, "rb").read()
+        hdr, cube = split_fits(raw, W, H, nb)
+        data = W * H * nb * 8
+        assert len(raw) == len(hdr) + (data + 2879) // 2880 * 2880
+        assert raw[len(hdr) + data:] == bytes(len(raw) - len(hdr) - data)
+        assert np.array_equal(cube.view(np.uint64), host.view(np.uint64))
+
+
 def test_fits_errors(grrt, need_gpu, tmp_path):
     """No bins, empty path or an unwritable path: -1 with the error text, as the reference."""
     R = grrt.Renderer(grrt.config_params(3, width=8, height=8))
